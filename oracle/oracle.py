@@ -1,0 +1,282 @@
+"""CPU oracle bindings -- TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper over ``oracle/_build/libmvp_oracle.so`` (the plain-C
+restatement of TenCirPauli's Rust MVP in ``oracle/mvp_oracle.c``).  Only the
+test-suite, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline and
+reference arms may import this module, and only as the checker or as the timed
+CPU baseline; the product library never calls it.
+
+Every function restates one reference item (paths inside the reference
+project ``crates/tencir-pauli-core/src``):
+
+* :func:`encode_codes`       -- ``word.rs:94-110`` (``PauliWord::from_codes``)
+* :func:`canonicalize`       -- ``operator.rs:117-155`` (``PauliOperator::from_terms``)
+* :func:`matrix_terms`       -- ``pauli_action.rs:24-88`` + ``hamiltonian.rs:564-571``
+* :func:`apply_term_direct`  -- ``hamiltonian.rs:204-270`` (TermDirect, lazy plan)
+* :func:`apply_xmask_diagonal` -- ``hamiltonian.rs:79-147,233-235`` (eager plan)
+* :func:`transition_count`   -- ``hamiltonian.rs:166-179``
+* :func:`apply_rows`         -- the TermDirect row loop on selected rows only
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libmvp_oracle.so")
+_lib: Optional[ctypes.CDLL] = None
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> str:
+    """Compile the oracle library with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def _load() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        lib = ctypes.CDLL(_LIB_PATH)
+        u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+        lib.oracle_encode_codes.argtypes = [u32, u64, _u8p, _u64p, _u64p]
+        lib.oracle_canonicalize.argtypes = [u32, u64, _u8p, _f64p, _u64p, _u64p, _f64p, _u64p, _u64p]
+        lib.oracle_matrix_terms.argtypes = [u32, u64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p]
+        lib.oracle_apply_term_direct.argtypes = [u32, u64, _u64p, _u64p, _f64p, _f64p, _f64p, i32]
+        lib.oracle_apply_rows.argtypes = [u32, u64, _u64p, _u64p, _f64p, _f64p, u64, _u64p, _f64p, i32]
+        lib.oracle_apply_xmask_diagonal.argtypes = [u32, u64, _u64p, _u64p, _f64p, _f64p, _f64p, _u64p, i32]
+        lib.oracle_transition_count.argtypes = [u32, u64, _u64p, _u64p, _f64p, _u64p, i32]
+        lib.oracle_group_count.argtypes = [u64, _u64p]
+        lib.oracle_group_count.restype = u64
+        lib.oracle_packed_word_count.argtypes = [u32]
+        lib.oracle_packed_word_count.restype = u32
+        lib.oracle_max_threads.restype = i32
+        for name in (
+            "oracle_encode_codes",
+            "oracle_canonicalize",
+            "oracle_matrix_terms",
+            "oracle_apply_term_direct",
+            "oracle_apply_rows",
+            "oracle_apply_xmask_diagonal",
+            "oracle_transition_count",
+        ):
+            getattr(lib, name).restype = i32
+        _lib = lib
+    return _lib
+
+
+def _p(array: np.ndarray, ptype):  # type: ignore[no-untyped-def]
+    return array.ctypes.data_as(ptype)
+
+
+class OracleError(RuntimeError):
+    def __init__(self, status: int, detail: str = "") -> None:
+        super().__init__(f"oracle status {status} {detail}".strip())
+        self.status = status
+
+
+def max_threads() -> int:
+    return int(_load().oracle_max_threads())
+
+
+def packed_word_count(nqubits: int) -> int:
+    return int(_load().oracle_packed_word_count(nqubits))
+
+
+def encode_codes(nqubits: int, codes: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    codes = np.ascontiguousarray(codes, dtype=np.uint8).reshape(-1, nqubits) if nqubits else np.zeros((len(codes), 0), np.uint8)
+    count = codes.shape[0]
+    width = packed_word_count(nqubits)
+    x = np.zeros((count, width), dtype=np.uint64)
+    z = np.zeros((count, width), dtype=np.uint64)
+    status = _load().oracle_encode_codes(nqubits, count, _p(codes, _u8p), _p(x, _u64p), _p(z, _u64p))
+    if status:
+        raise OracleError(status)
+    return x, z
+
+
+def canonicalize(
+    nqubits: int, codes: np.ndarray, coefficients: np.ndarray
+) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Return canonical (x_words[T,W], z_words[T,W], coefficients[T])."""
+    count = len(coefficients)
+    codes = np.ascontiguousarray(np.asarray(codes, dtype=np.uint8).reshape(count, nqubits))
+    coeffs = np.ascontiguousarray(np.asarray(coefficients, dtype=np.complex128))
+    width = packed_word_count(nqubits)
+    x = np.zeros((max(count, 1), width), dtype=np.uint64)
+    z = np.zeros((max(count, 1), width), dtype=np.uint64)
+    out = np.zeros(max(count, 1), dtype=np.complex128)
+    n_out = np.zeros(1, dtype=np.uint64)
+    bad = np.zeros(1, dtype=np.uint64)
+    status = _load().oracle_canonicalize(
+        nqubits,
+        count,
+        _p(codes, _u8p),
+        _p(coeffs.view(np.float64), _f64p),
+        _p(x, _u64p),
+        _p(z, _u64p),
+        _p(out.view(np.float64), _f64p),
+        _p(n_out, _u64p),
+        _p(bad, _u64p),
+    )
+    if status:
+        raise OracleError(status, f"index {int(bad[0])}")
+    t = int(n_out[0])
+    return x[:t].copy(), z[:t].copy(), out[:t].copy()
+
+
+def matrix_terms(
+    nqubits: int, x_words: np.ndarray, z_words: np.ndarray, coefficients: np.ndarray
+) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Return (x_mask, z_mask, weighted_phase) in the MSB matrix index space."""
+    count = len(coefficients)
+    xw = np.ascontiguousarray(x_words, dtype=np.uint64)
+    zw = np.ascontiguousarray(z_words, dtype=np.uint64)
+    coeffs = np.ascontiguousarray(coefficients, dtype=np.complex128)
+    xm = np.zeros(max(count, 1), dtype=np.uint64)
+    zm = np.zeros(max(count, 1), dtype=np.uint64)
+    wp = np.zeros(max(count, 1), dtype=np.complex128)
+    status = _load().oracle_matrix_terms(
+        nqubits,
+        count,
+        _p(xw, _u64p),
+        _p(zw, _u64p),
+        _p(coeffs.view(np.float64), _f64p),
+        _p(xm, _u64p),
+        _p(zm, _u64p),
+        _p(wp.view(np.float64), _f64p),
+    )
+    if status:
+        raise OracleError(status)
+    return xm[:count].copy(), zm[:count].copy(), wp[:count].copy()
+
+
+def apply_term_direct(
+    nqubits: int,
+    x_mask: np.ndarray,
+    z_mask: np.ndarray,
+    weighted: np.ndarray,
+    state: np.ndarray,
+    threads: int = 0,
+) -> np.ndarray:
+    state = np.ascontiguousarray(state, dtype=np.complex128)
+    if state.shape != (1 << nqubits,):
+        raise ValueError("state length must be 2**nqubits")
+    out = np.empty_like(state)
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    zm = np.ascontiguousarray(z_mask, dtype=np.uint64)
+    wp = np.ascontiguousarray(weighted, dtype=np.complex128)
+    status = _load().oracle_apply_term_direct(
+        nqubits,
+        len(wp),
+        _p(xm, _u64p),
+        _p(zm, _u64p),
+        _p(wp.view(np.float64), _f64p),
+        _p(state.view(np.float64), _f64p),
+        _p(out.view(np.float64), _f64p),
+        threads,
+    )
+    if status:
+        raise OracleError(status)
+    return out
+
+
+def apply_rows(
+    nqubits: int,
+    x_mask: np.ndarray,
+    z_mask: np.ndarray,
+    weighted: np.ndarray,
+    state: np.ndarray,
+    rows: np.ndarray,
+    threads: int = 0,
+) -> np.ndarray:
+    state = np.ascontiguousarray(state, dtype=np.complex128)
+    rows = np.ascontiguousarray(rows, dtype=np.uint64)
+    if rows.size and int(rows.max()) >= (1 << nqubits):
+        raise ValueError("row index out of range")
+    out = np.empty(len(rows), dtype=np.complex128)
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    zm = np.ascontiguousarray(z_mask, dtype=np.uint64)
+    wp = np.ascontiguousarray(weighted, dtype=np.complex128)
+    status = _load().oracle_apply_rows(
+        nqubits,
+        len(wp),
+        _p(xm, _u64p),
+        _p(zm, _u64p),
+        _p(wp.view(np.float64), _f64p),
+        _p(state.view(np.float64), _f64p),
+        len(rows),
+        _p(rows, _u64p),
+        _p(out.view(np.float64), _f64p),
+        threads,
+    )
+    if status:
+        raise OracleError(status)
+    return out
+
+
+def apply_xmask_diagonal(
+    nqubits: int,
+    x_mask: np.ndarray,
+    z_mask: np.ndarray,
+    weighted: np.ndarray,
+    state: np.ndarray,
+    threads: int = 0,
+) -> Tuple[np.ndarray, int]:
+    state = np.ascontiguousarray(state, dtype=np.complex128)
+    out = np.empty_like(state)
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    zm = np.ascontiguousarray(z_mask, dtype=np.uint64)
+    wp = np.ascontiguousarray(weighted, dtype=np.complex128)
+    transitions = np.zeros(1, dtype=np.uint64)
+    status = _load().oracle_apply_xmask_diagonal(
+        nqubits,
+        len(wp),
+        _p(xm, _u64p),
+        _p(zm, _u64p),
+        _p(wp.view(np.float64), _f64p),
+        _p(state.view(np.float64), _f64p),
+        _p(out.view(np.float64), _f64p),
+        _p(transitions, _u64p),
+        threads,
+    )
+    if status:
+        raise OracleError(status)
+    return out, int(transitions[0])
+
+
+def transition_count(
+    nqubits: int, x_mask: np.ndarray, z_mask: np.ndarray, weighted: np.ndarray, threads: int = 0
+) -> int:
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    zm = np.ascontiguousarray(z_mask, dtype=np.uint64)
+    wp = np.ascontiguousarray(weighted, dtype=np.complex128)
+    out = np.zeros(1, dtype=np.uint64)
+    status = _load().oracle_transition_count(
+        nqubits, len(wp), _p(xm, _u64p), _p(zm, _u64p), _p(wp.view(np.float64), _f64p), _p(out, _u64p), threads
+    )
+    if status:
+        raise OracleError(status)
+    return int(out[0])
+
+
+def group_count(x_mask: np.ndarray) -> int:
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    return int(_load().oracle_group_count(len(xm), _p(xm, _u64p)))
+
+
+def mvp(nqubits: int, codes: np.ndarray, coefficients: np.ndarray, state: np.ndarray, threads: int = 0) -> np.ndarray:
+    """One-shot ``PauliOperator::mvp`` (hamiltonian.rs:481-483): canonicalize, compile, apply."""
+    xw, zw, c = canonicalize(nqubits, codes, coefficients)
+    xm, zm, wp = matrix_terms(nqubits, xw, zw, c)
+    return apply_term_direct(nqubits, xm, zm, wp, state, threads)

@@ -1,0 +1,145 @@
+"""Generate the golden MVP fixtures in this folder.
+
+Run in a container where the TenCirPauli reference checkout is present:
+
+    python tests/golden/make_golden.py /path/to/TenCirPauli
+
+The expected outputs come from the reference's own independent dense oracle
+``tests/reference.py`` (Kronecker products of the Pauli matrices, qubit 0 as
+the most significant bit), imported from the reference checkout, and from the
+fixed vectors written in the reference's tests.  The inputs replicate the
+random streams of the reference tests that pin the MVP path:
+
+* ``tests/test_hamiltonian.py:15-24,51-68``  make_operator(n), n in {0,1,2,5}
+* ``tests/test_hamiltonian.py:126-147``       random complex differential, n=0..6
+* ``tests/test_hamiltonian.py:71-77``         first/last qubit ordering
+* ``tests/test_native_abi.py:84-120``         H = 2Z + I, apply([1,2]) == [3,-2]
+* ``tests/test_pauli_operator.py:23-30,223-238`` canonical order / aggregation
+* ``crates/tencir-pauli-core/src/tests.rs:25-37,121-158`` mvp_test_operator
+
+Only the fixtures are committed; the tests never read the reference checkout.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _codes_from_string(word: str) -> tuple:
+    return tuple("IXYZ".index(ch) for ch in word)
+
+
+def main(reference_root: str) -> None:
+    sys.path.insert(0, os.path.join(reference_root, "tests"))
+    from reference import dense_operator  # the reference's independent oracle
+
+    out = {}
+
+    # make_operator (test_hamiltonian.py:15-24) for n in (0, 1, 2, 5)
+    for n in (0, 1, 2, 5):
+        structures = [
+            tuple((index + qubit) % 4 for qubit in range(n))
+            for index in range(min(10, 4**n))
+        ]
+        coefficients = [complex(index + 1, -index / 3) for index in range(len(structures))]
+        state = np.arange(1 << n, dtype=np.float64) + 1j * np.arange(1 << n)
+        dense = dense_operator(n, structures, coefficients)
+        out[f"make_operator_{n}"] = dict(
+            nqubits=np.int64(n),
+            codes=np.asarray(structures, dtype=np.uint8).reshape(len(structures), n),
+            coefficients=np.asarray(coefficients, dtype=np.complex128),
+            state=state,
+            expected=dense @ state,
+        )
+
+    # random complex differential (test_hamiltonian.py:126-147), same RNG stream
+    rng = np.random.default_rng(20260801)
+    for n in range(7):
+        structures = tuple(
+            tuple(int(value) for value in rng.integers(0, 4, size=n)) for _ in range(24)
+        )
+        coefficients = tuple(
+            complex(float(re), float(im)) for re, im in rng.normal(size=(24, 2))
+        )
+        state = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+        dense = dense_operator(n, structures, coefficients)
+        out[f"random_differential_{n}"] = dict(
+            nqubits=np.int64(n),
+            codes=np.asarray(structures, dtype=np.uint8).reshape(24, n),
+            coefficients=np.asarray(coefficients, dtype=np.complex128),
+            state=state,
+            expected=dense @ state,
+        )
+
+    # qubit ordering (test_hamiltonian.py:71-77): one term on qubit 0 or qubit 2
+    for code in (1, 2, 3):
+        for name, codes in (("first", (code, 0, 0)), ("last", (0, 0, code))):
+            dense = dense_operator(3, (codes,), (1.0,))
+            state = np.arange(8, dtype=np.float64) + 0.5j * np.arange(8)[::-1]
+            out[f"ordering_{name}_{code}"] = dict(
+                nqubits=np.int64(3),
+                codes=np.asarray([codes], dtype=np.uint8),
+                coefficients=np.asarray([1.0], dtype=np.complex128),
+                state=state,
+                expected=dense @ state,
+            )
+
+    # ABI fixed vector (test_native_abi.py:84-120): H = 2Z + I on one qubit
+    out["abi_fixed"] = dict(
+        nqubits=np.int64(1),
+        codes=np.asarray([_codes_from_string("Z"), _codes_from_string("I")], dtype=np.uint8),
+        coefficients=np.asarray([2.0, 1.0], dtype=np.complex128),
+        state=np.asarray([1.0, 2.0], dtype=np.complex128),
+        expected=np.asarray([3.0, -2.0], dtype=np.complex128),
+    )
+
+    # mvp_test_operator (tests.rs:25-37) at (1 qubit, 1 term) and (10, 64),
+    # with the states of tests.rs:123,140-143
+    for n, t in ((1, 1), (10, 64)):
+        structures = [
+            tuple(int(bool(mask & (1 << q))) for q in range(n)) for mask in range(t)
+        ]
+        coefficients = [complex(index + 1.0, -index * 0.25) for index in range(t)]
+        if n == 1:
+            state = np.asarray([3.0 - 2.0j, 5.0 + 4.0j])
+        else:
+            index = np.arange(1 << n, dtype=np.float64)
+            state = index * 0.5 + 1j * (1.0 - index * 0.125)
+        dense = dense_operator(n, structures, coefficients)
+        out[f"rust_fixture_{n}_{t}"] = dict(
+            nqubits=np.int64(n),
+            codes=np.asarray(structures, dtype=np.uint8).reshape(t, n),
+            coefficients=np.asarray(coefficients, dtype=np.complex128),
+            state=state,
+            expected=dense @ state,
+        )
+
+    for name, fields in out.items():
+        np.savez(os.path.join(HERE, f"{name}.npz"), **fields)
+
+    # canonicalization known answers written in the reference tests
+    np.savez(
+        os.path.join(HERE, "canonical_known_answers.npz"),
+        # test_pauli_operator.py:23-30
+        a_codes=np.asarray(
+            [_codes_from_string(w) for w in ("ZX", "II", "ZX", "II")], dtype=np.uint8
+        ),
+        a_coefficients=np.asarray([1.0, 2.0, -0.25j, -2.0], dtype=np.complex128),
+        a_expected_codes=np.asarray([_codes_from_string("ZX")], dtype=np.uint8),
+        a_expected_coefficients=np.asarray([1.0 - 0.25j], dtype=np.complex128),
+        # test_pauli_operator.py:223-238
+        b_codes=np.asarray([[3, 1], [0, 0], [3, 1]], dtype=np.uint8),
+        b_coefficients=np.asarray([1.0, 2.0, -0.25j], dtype=np.complex128),
+        b_expected_codes=np.asarray([[0, 0], [3, 1]], dtype=np.uint8),
+        b_expected_coefficients=np.asarray([2.0, 1.0 - 0.25j], dtype=np.complex128),
+    )
+    print(f"wrote {len(out) + 1} fixtures to {HERE}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
