@@ -1,0 +1,434 @@
+"""Benchmark of the B200 matrix-free Pauli MVP (one JSON line on rank 0).
+
+Workload (default): the random 2..4-local Hamiltonian on n = 28 qubits --
+2,000 raw words (weight uniform in {2,3,4} on distinct uniformly random
+qubits, letters uniform over X/Y/Z, real N(0,1) coefficients, seed 20261203),
+canonicalized -- applied to a complex128 statevector (re/im i.i.d. N(0,1),
+L2-normalised).  A step is one y = H x over the whole 2^28 state.
+
+Metric: amplitude-terms/s = T_canonical * 2^n * (vectors per step) / step time.
+``value`` is device time (CUDA events on the launching stream, inputs resident
+in HBM, 4 GiB vectors > L2 so no flush is needed); ``e2e`` is the same metric
+through the public host ``apply_into`` path (pinned host buffers, H2D + kernel
++ D2H in every step).  ``--impl reference`` times the reference's CPU
+algorithm (the C restatement of the Rust TermDirect loop, all host cores) on a
+bounded row sample of the same workload.
+
+Multi-GPU (``torchrun --nproc-per-node N``): one independent state per rank
+(weak scaling, no collective on the data path); the step time is the max over
+ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from typing import Any, Dict, List, Optional
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MVP amplitude-terms/s"
+UNIT = "amp-terms/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _measured_peaks() -> Dict[str, Any]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            data = json.load(fh)
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": FALLBACK_HBM_GBS, "source": "fallback"}
+
+
+def _profile_traffic(kernel: str) -> Optional[float]:
+    """Per-launch DRAM bytes from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, device_index: int) -> None:
+        self.device_index = device_index
+        self.proc: Optional[subprocess.Popen] = None
+        self.path = tempfile.mktemp(prefix="tcp_clocks_", suffix=".csv")
+
+    def start(self) -> None:
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                [
+                    "nvidia-smi",
+                    f"--id={self.device_index}",
+                    f"--query-gpu={self.FIELDS}",
+                    "--format=csv,noheader,nounits",
+                    "-lms",
+                    "200",
+                ],
+                stdout=self.fh,
+                stderr=subprocess.DEVNULL,
+            )
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> Dict[str, Any]:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm: List[float] = []
+        smax: List[float] = []
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def _smi_id(device: int) -> str:
+    """nvidia-smi --id for a torch ordinal (PCI bus id: robust to CUDA_VISIBLE_DEVICES)."""
+    import torch
+
+    props = torch.cuda.get_device_properties(device)
+    try:
+        return f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+    except AttributeError:
+        return str(device)
+
+
+def build_operator(args: argparse.Namespace):
+    from tencirpauli_b200 import PauliOperator, workloads
+
+    codes, coeffs = workloads.random_k_local(n=args.nqubits, words=args.words, seed=args.seed)
+    return PauliOperator.from_code_arrays(codes, coeffs)
+
+
+def cpu_reference_rate(op, state_host: np.ndarray, seconds: float, threads: int = 0) -> Dict[str, Any]:
+    """The C restatement of the reference's Rust/rayon TermDirect row loop
+    (crates/tencir-pauli-core/src/hamiltonian.rs:204-270) on a random row
+    sample sized to about ``seconds`` of CPU work."""
+    from oracle import oracle
+
+    n = op.nqubits
+    xm, zm, wp = oracle.matrix_terms(n, op.x_words, op.z_words, op.coefficients)
+    rng = np.random.default_rng(1)
+    cores = threads or oracle.max_threads()
+    dim = 1 << n
+
+    # Contiguous row blocks, as rayon's par_iter_mut walks rows in order.
+    def block(count: int) -> np.ndarray:
+        start = int(rng.integers(0, max(1, dim - count + 1)))
+        return np.arange(start, start + count, dtype=np.uint64)
+
+    probe = block(min(dim, 1 << 14))
+    t0 = time.perf_counter()
+    oracle.apply_rows(n, xm, zm, wp, state_host, probe, cores)
+    dt = max(time.perf_counter() - t0, 1e-6)
+    per_row = dt / probe.size
+    rows = int(min(dim, max(probe.size, seconds / per_row)))
+    sample = block(rows)
+    t0 = time.perf_counter()
+    oracle.apply_rows(n, xm, zm, wp, state_host, sample, cores)
+    dt = time.perf_counter() - t0
+    rate = op.term_count * rows / dt
+    return {
+        "value": rate,
+        "unit": UNIT,
+        "cores": cores,
+        "kind": "port",
+        "sample": f"{rows} consecutive rows of the 2^{n} state x {op.term_count} terms "
+        f"(TermDirect row loop, {dt:.1f} s)",
+        "seconds": dt,
+    }
+
+
+def run_reference(args: argparse.Namespace) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    op = build_operator(args)
+    n = op.nqubits
+    rng = np.random.default_rng(args.seed)
+    state = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    state /= np.linalg.norm(state)
+    cores = oracle.max_threads()
+    for _ in range(args.warmup):
+        cpu_reference_rate(op, state, seconds=0.5, threads=cores)
+    rates = []
+    samples = []
+    for _ in range(args.steps):
+        r = cpu_reference_rate(op, state, seconds=args.reference_seconds, threads=cores)
+        rates.append(r["value"])
+        samples.append(r)
+    value = float(statistics.median(rates))
+    amp_terms_per_step = op.term_count * (1 << n)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 * amp_terms_per_step / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": workload_config(args, op),
+        "cpu_baseline": {
+            "value": value,
+            "unit": UNIT,
+            "cores": cores,
+            "kind": "port",
+            "sample": samples[-1]["sample"] + "; C restatement of the reference Rust MVP (Rust build unavailable)",
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args: argparse.Namespace, op) -> Dict[str, Any]:
+    return {
+        "workload": f"random {args.words}-word 2..4-local Hamiltonian, n={args.nqubits}",
+        "nqubits": args.nqubits,
+        "raw_words": args.words,
+        "terms": op.term_count,
+        "seed": args.seed,
+        "state": "complex128" if args.dtype == "c128" else "complex64",
+        "vectors_per_step_per_gpu": 1,
+        "l2": "inputs larger than L2 (4 GiB per vector), no flush",
+    }
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--nqubits", type=int, default=28)
+    parser.add_argument("--words", type=int, default=2000)
+    parser.add_argument("--seed", type=int, default=20261203)
+    parser.add_argument("--dtype", choices=["c128", "c64"], default="c128")
+    parser.add_argument("--e2e-steps", type=int, default=3)
+    parser.add_argument("--cpu-seconds", type=float, default=15.0)
+    parser.add_argument("--reference-seconds", type=float, default=10.0)
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from tencirpauli_b200 import workloads
+
+    op = build_operator(args)
+    plan = op.native_mvp_plan()
+    n = op.nqubits
+    T = op.term_count
+    dim = 1 << n
+    cdtype = torch.complex128 if args.dtype == "c128" else torch.complex64
+    elem = 16 if args.dtype == "c128" else 8
+    x = workloads.random_state_device(n, seed=args.seed + rank, dtype=cdtype)
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        plan.apply_device(x, y, stream)
+    torch.cuda.synchronize()
+    plan._native_plan.device_status()
+
+    sampler = ClockSampler(_smi_id(torch.cuda.current_device()))
+    sampler.start()
+    time.sleep(0.3)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_begin.record(stream)
+    for k in range(args.steps):
+        starts[k].record(stream)
+        plan.apply_device(x, y, stream)
+        ends[k].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    plan._native_plan.device_status()
+    total_ms = t_begin.elapsed_time(t_end)
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_local = total_ms / args.steps
+    ms_tensor = torch.tensor([ms_local], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_tensor, op=dist.ReduceOp.MAX)
+    ms_per_step = float(ms_tensor.item())
+    amp_terms = T * dim
+    value = amp_terms * world / (ms_per_step / 1000.0)
+
+    # end to end through the public host apply_into (pinned host buffers)
+    x_host = torch.empty(dim, dtype=cdtype, pin_memory=True)
+    y_host = torch.empty(dim, dtype=cdtype, pin_memory=True)
+    x_host.copy_(x)
+    xh = x_host.numpy()
+    yh = y_host.numpy()
+    native = plan._native_plan
+    if args.dtype == "c128":
+        host_apply = lambda: native.apply_into(xh, yh, 2**63 - 1)  # noqa: E731
+    else:
+        host_apply = lambda: native.apply_c64_into(xh, yh)  # noqa: E731
+    host_apply()
+    e2e_times = []
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        host_apply()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_local = statistics.median(e2e_times)
+    e2e_tensor = torch.tensor([e2e_local], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_tensor, op=dist.ReduceOp.MAX)
+    e2e_value = amp_terms * world / float(e2e_tensor.item())
+
+    # accuracy of this run's result on a row sample (rank 0), vs the oracle
+    line: Dict[str, Any] = {}
+    if rank == 0:
+        peaks = _measured_peaks()
+        kern_ms = statistics.mean(kernel_ms)
+        b_alg = dim * 2 * elem
+        achieved = b_alg / (kern_ms / 1000.0) / 1e9
+        kernel_name = "k_tiled<3,double>" if args.dtype == "c128" else "k_tiled<4,float>"
+        traffic = _profile_traffic(kernel_name)
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.dtype == "c128" else "f32",
+            "data": "synthetic",
+            "config": workload_config(args, op),
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peaks["hbm_gbs"],
+                "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": traffic,
+                "peak_source": peaks["source"],
+                "kernel": kernel_name,
+                "bytes_per_launch": b_alg,
+                "kernel_ms": kern_ms,
+            },
+            "e2e": {
+                "value": e2e_value,
+                "unit": UNIT,
+                "h2d_bytes_per_step": dim * elem,
+                "d2h_bytes_per_step": dim * elem,
+                "ms_per_step": 1000.0 * float(e2e_tensor.item()),
+            },
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "plan": {
+                "groups": plan.group_count,
+                "tile_bits": int(native.info.tile_bits_c128 if args.dtype == "c128" else native.info.tile_bits_c64),
+                "steps": int(native.info.steps_c128 if args.dtype == "c128" else native.info.steps_c64),
+            },
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            state_host = x_host.numpy() if args.dtype == "c128" else x_host.numpy().astype(np.complex128)
+            cb = cpu_reference_rate(op, state_host, seconds=args.cpu_seconds)
+            cb.pop("seconds", None)
+            line["cpu_baseline"] = cb
+        # row-sample accuracy against the oracle (the checker)
+        from oracle import oracle
+
+        rows = np.sort(np.random.default_rng(3).choice(dim, size=2048, replace=False)).astype(np.uint64)
+        xm, zm, wp = oracle.matrix_terms(n, op.x_words, op.z_words, op.coefficients)
+        state_host = x_host.numpy().astype(np.complex128)
+        ref = oracle.apply_rows(n, xm, zm, wp, state_host, rows)
+        got = y[torch.from_numpy(rows.astype(np.int64)).cuda()].cpu().numpy().astype(np.complex128)
+        line["accuracy"] = {
+            "rows_checked": int(rows.size),
+            "rel_err_vs_oracle": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

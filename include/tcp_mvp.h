@@ -1,0 +1,178 @@
+/*
+ * tcp_mvp.h -- C ABI of the B200 (sm_100a) matrix-free Pauli MVP library
+ * `libtcpmvp.so`.
+ *
+ * The library computes y = sum_k c_k P_k x over a 2^n complex statevector for
+ * a canonical Pauli operator, the path behind TenCirPauli's
+ * `PauliOperator.native_mvp_plan()` / `.mvp()`.  Every entry point returns an
+ * `int` status (TCP_OK == 0) and never aborts; `tcp_last_error` returns the
+ * calling thread's last message.  No torch or CUDA-runtime C++ types appear in
+ * the signatures: CUDA streams travel as `void*` (a `cudaStream_t`).
+ *
+ * Conventions (identical to the reference, paths inside the reference project):
+ *  - packed words: qubit q is bit q%64 of word q/64
+ *    (crates/tencir-pauli-core/src/word.rs:94-110);
+ *  - codes 0=I 1=X 2=Y 3=Z (word.rs:296-304);
+ *  - state index: qubit 0 is the most significant bit, matrix bit of qubit q
+ *    is 1 << (n-1-q) (crates/tencir-pauli-core/src/pauli_action.rs:65);
+ *  - y[r] = sum_k c_k i^{#Y_k} (-1)^{popcount(z_k & (r ^ x_k))} x[r ^ x_k]
+ *    (crates/tencir-pauli-core/src/hamiltonian.rs:238-243);
+ *  - complex128 buffers are interleaved (re, im) doubles, complex64 buffers
+ *    interleaved floats.
+ */
+#ifndef TCP_MVP_H
+#define TCP_MVP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCP_ABI_VERSION 1
+
+/* Status codes.  1..10 mirror the PauliError variants used on this path
+ * (crates/tencir-pauli-core/src/error.rs:5-74), in declaration order. */
+enum tcp_status {
+    TCP_OK = 0,
+    TCP_ERR_INVALID_CODE = 1,             /* PauliError::InvalidCode */
+    TCP_ERR_INVALID_WORD_LENGTH = 2,      /* PauliError::InvalidWordLength */
+    TCP_ERR_INCOMPATIBLE_QUBITS = 3,      /* PauliError::IncompatibleQubitCounts */
+    TCP_ERR_INVALID_STRUCTURE_LENGTH = 4, /* PauliError::InvalidStructureLength */
+    TCP_ERR_NON_FINITE_COEFFICIENT = 5,   /* PauliError::NonFiniteCoefficient */
+    TCP_ERR_NON_CANONICAL_TERMS = 7,      /* PauliError::NonCanonicalTerms */
+    TCP_ERR_OVERFLOW = 8,                 /* PauliError::Overflow */
+    TCP_ERR_MEMORY_LIMIT = 9,             /* PauliError::MemoryLimit */
+    TCP_ERR_INVALID_SECTOR = 10,          /* PauliError::InvalidSector (bad storage label) */
+    /* Library-specific statuses. */
+    TCP_ERR_INVALID_ARGUMENT = 32, /* null pointer, bad enum, overlapping buffers */
+    TCP_ERR_CUDA = 33,             /* a CUDA runtime call failed */
+    TCP_ERR_DEVICE_TIMEOUT = 34,   /* a bounded device-side wait expired */
+    TCP_ERR_ALLOCATION = 35,       /* device or host allocation failed */
+    TCP_ERR_WRONG_DEVICE = 36      /* plan used on a device other than its own */
+};
+
+enum tcp_storage {
+    TCP_STORAGE_LAZY = 0, /* MvpStrategy::TermDirect label (hamiltonian.rs:63-76) */
+    TCP_STORAGE_EAGER = 1 /* MvpStrategy::XMaskDiagonal label (hamiltonian.rs:79-147) */
+};
+
+enum tcp_dtype {
+    TCP_DTYPE_C128 = 0, /* complex128 state, FP64 arithmetic */
+    TCP_DTYPE_C64 = 1   /* complex64 state, FP32 products, Kahan sum over groups */
+};
+
+/* Opaque, immutable-after-create plan.  Thread-safe for concurrent apply. */
+typedef struct tcp_mvp_plan tcp_mvp_plan;
+
+typedef struct tcp_mvp_plan_info_t {
+    uint32_t nqubits;
+    uint32_t word_count;
+    uint64_t dimension;        /* 2^n */
+    uint64_t term_count;       /* canonical terms held by the plan */
+    uint64_t group_count;      /* distinct x masks */
+    int32_t storage;           /* enum tcp_storage */
+    int32_t device;            /* CUDA ordinal the plan lives on */
+    int64_t transition_count;  /* eager nonzero count, -1 for lazy plans (None) */
+    uint64_t device_bytes;     /* device memory retained by the plan */
+    uint32_t tile_bits_c128;   /* tile width (log2 rows) of the c128 schedule */
+    uint32_t tile_bits_c64;    /* tile width (log2 rows) of the c64 schedule */
+    uint64_t steps_c128;       /* outer tile patterns in the c128 schedule */
+    uint64_t steps_c64;
+} tcp_mvp_plan_info_t;
+
+/* Library version (TCP_ABI_VERSION) */
+int tcp_abi_version(void);
+
+/* Copy the calling thread's last error message (NUL-terminated, truncated to
+ * `capacity`).  Returns the full message length. */
+size_t tcp_last_error(char *buffer, size_t capacity);
+
+/*
+ * Canonicalize a term batch: replaces PauliOperator::from_terms
+ * (crates/tencir-pauli-core/src/operator.rs:117-155) and the PyO3 entry
+ * `pauli_operator_native_array` (crates/tencirpauli-native/src/operator.rs:205-243).
+ * codes: uint8[count * nqubits] (0..3); coefficients: double[2*count] (re, im).
+ * Duplicate words are summed in ascending (re bits, im bits) order from 0+0i,
+ * exact zeros are dropped, words are sorted by their code tuple.
+ * Outputs (capacity `count` terms): out_x/out_z uint64[count * word_count],
+ * out_coefficients double[2*count]; *out_count receives the canonical count.
+ * On TCP_ERR_INVALID_CODE / TCP_ERR_NON_FINITE_COEFFICIENT, *bad_index (if
+ * non-null) receives the offending qubit / term index.
+ */
+int tcp_pauli_canonicalize(uint32_t nqubits, uint64_t count, const uint8_t *codes,
+                           const double *coefficients, uint64_t *out_x, uint64_t *out_z,
+                           double *out_coefficients, uint64_t *out_count, uint64_t *bad_index);
+
+/*
+ * Build a plan on the current CUDA device.  Replaces MvpPlan::from_operator
+ * (storage LAZY, hamiltonian.rs:63-76) and MvpPlan::from_operator_reusable
+ * (storage EAGER, hamiltonian.rs:79-147), reached from the PyO3 entry
+ * `pauli_mvp_plan_handle` (crates/tencirpauli-native/src/hamiltonian.rs:98-116).
+ * x_words / z_words: uint64[term_count * word_count], coefficients:
+ * double[2*term_count]; the term list is the canonical operator's.
+ * max_bytes is the reference's eager construction budget (u128 there; here
+ * UINT64_MAX means unlimited); lazy plans ignore it.
+ */
+int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32_t word_count,
+                        const uint64_t *x_words, const uint64_t *z_words,
+                        const double *coefficients, int storage, uint64_t max_bytes,
+                        tcp_mvp_plan **out_plan);
+
+/* Release a plan and its device memory.  NULL is accepted. */
+int tcp_mvp_plan_destroy(tcp_mvp_plan *plan);
+
+/* Metadata: nqubits / term_count / transition_count mirror the getters of
+ * MvpPlan (hamiltonian.rs:149-179) and the PyO3 NativeMvpPlan properties. */
+int tcp_mvp_plan_info(const tcp_mvp_plan *plan, tcp_mvp_plan_info_t *info);
+
+/*
+ * Drop-in for MvpPlan::apply_into (hamiltonian.rs:204-270) and the PyO3
+ * NativeMvpPlan.apply_into (crates/tencirpauli-native/src/hamiltonian.rs:176-193):
+ * host complex128 buffers, blocking.  Copies `state` to the device, applies,
+ * copies the result back and overwrites every element of `result`.
+ * Lengths are in complex elements; a length other than 2^n returns
+ * TCP_ERR_INVALID_STRUCTURE_LENGTH ("expected structure length E, got A").
+ * max_bytes is accepted and ignored, as in the reference (hamiltonian.rs:223).
+ */
+int tcp_mvp_apply_into_host(const tcp_mvp_plan *plan, const double *state, uint64_t state_len,
+                            double *result, uint64_t result_len, uint64_t max_bytes);
+
+/* Same, complex64 host buffers (FP32 arithmetic with Kahan group sums). */
+int tcp_mvp_apply_into_host_c64(const tcp_mvp_plan *plan, const float *state,
+                                uint64_t state_len, float *result, uint64_t result_len);
+
+/*
+ * Device-resident apply, asynchronous on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream).  d_state / d_result hold `nrhs` vectors of
+ * `len` == 2^n complex elements each, vector v at offset v * len.  dtype is
+ * enum tcp_dtype.  Buffers must not overlap.  Device-side timeouts are
+ * reported by tcp_mvp_plan_device_status after the stream is synchronised.
+ */
+int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
+                              uint64_t len, uint32_t nrhs, int dtype, void *stream);
+
+/* Synchronise the plan's device and report (then clear) any device-side error
+ * flag raised by kernels of this plan. */
+int tcp_mvp_plan_device_status(const tcp_mvp_plan *plan);
+
+/*
+ * Eager transition count on the device: the number of nonzero entries of the
+ * per-x-mask diagonals D_m[c] = sum_{k in m} w_k (-1)^{popcount(z_k & c)}
+ * summed in canonical term order (hamiltonian.rs:121-139,166-179).
+ */
+int tcp_mvp_transition_count(const tcp_mvp_plan *plan, uint64_t *out_count);
+
+/*
+ * Diagonal extraction: writes H_ii (the x_mask == 0 group, complex128) for
+ * every basis state into d_diag (2^n elements), asynchronous on `stream`.
+ * Used by Jacobi-type preconditioners.
+ */
+int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, uint64_t len, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCP_MVP_H */

@@ -1,0 +1,405 @@
+"""ctypes binding of ``libtcpmvp.so`` (the C ABI declared in ``include/tcp_mvp.h``).
+
+This module is the process-internal boundary that replaces the reference's
+PyO3 extension ``tencirpauli._native`` for the MVP path
+(``crates/tencirpauli-native/src/hamiltonian.rs:31-194`` and
+``crates/tencirpauli-native/src/operator.rs:164-267``).  It loads the in-tree
+CUDA library and fails loudly when it is missing: there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+import threading
+from typing import Any, Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "_lib", "libtcpmvp.so")
+
+# Status codes of include/tcp_mvp.h
+TCP_OK = 0
+TCP_ERR_INVALID_CODE = 1
+TCP_ERR_INVALID_WORD_LENGTH = 2
+TCP_ERR_INCOMPATIBLE_QUBITS = 3
+TCP_ERR_INVALID_STRUCTURE_LENGTH = 4
+TCP_ERR_NON_FINITE_COEFFICIENT = 5
+TCP_ERR_NON_CANONICAL_TERMS = 7
+TCP_ERR_OVERFLOW = 8
+TCP_ERR_MEMORY_LIMIT = 9
+TCP_ERR_INVALID_SECTOR = 10
+TCP_ERR_INVALID_ARGUMENT = 32
+TCP_ERR_CUDA = 33
+TCP_ERR_DEVICE_TIMEOUT = 34
+TCP_ERR_ALLOCATION = 35
+TCP_ERR_WRONG_DEVICE = 36
+
+TCP_STORAGE_LAZY = 0
+TCP_STORAGE_EAGER = 1
+TCP_DTYPE_C128 = 0
+TCP_DTYPE_C64 = 1
+
+U64_MAX = (1 << 64) - 1
+
+# Every symbol include/tcp_mvp.h declares.
+EXPORTED_SYMBOLS = (
+    "tcp_abi_version",
+    "tcp_last_error",
+    "tcp_pauli_canonicalize",
+    "tcp_mvp_plan_create",
+    "tcp_mvp_plan_destroy",
+    "tcp_mvp_plan_info",
+    "tcp_mvp_apply_into_host",
+    "tcp_mvp_apply_into_host_c64",
+    "tcp_mvp_apply_into_device",
+    "tcp_mvp_plan_device_status",
+    "tcp_mvp_transition_count",
+    "tcp_mvp_diagonal_device",
+)
+
+
+class TcpPlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("nqubits", ctypes.c_uint32),
+        ("word_count", ctypes.c_uint32),
+        ("dimension", ctypes.c_uint64),
+        ("term_count", ctypes.c_uint64),
+        ("group_count", ctypes.c_uint64),
+        ("storage", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("transition_count", ctypes.c_int64),
+        ("device_bytes", ctypes.c_uint64),
+        ("tile_bits_c128", ctypes.c_uint32),
+        ("tile_bits_c64", ctypes.c_uint32),
+        ("steps_c128", ctypes.c_uint64),
+        ("steps_c64", ctypes.c_uint64),
+    ]
+
+
+_lib: Optional[ctypes.CDLL] = None
+_lib_lock = threading.Lock()
+
+
+def load_library() -> ctypes.CDLL:
+    """Load the in-tree CUDA library; raise ImportError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIBRARY_PATH):
+            raise ImportError(
+                f"libtcpmvp.so is not built ({LIBRARY_PATH}); run "
+                "`python -m tencirpauli_b200.build` (the MVP has no CPU fallback)"
+            )
+        lib = ctypes.CDLL(LIBRARY_PATH)
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        f64p = ctypes.POINTER(ctypes.c_double)
+        f32p = ctypes.POINTER(ctypes.c_float)
+        vp = ctypes.c_void_p
+        u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+        lib.tcp_abi_version.restype = i32
+        lib.tcp_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        lib.tcp_last_error.restype = ctypes.c_size_t
+        lib.tcp_pauli_canonicalize.argtypes = [u32, u64, u8p, f64p, u64p, u64p, f64p, u64p, u64p]
+        lib.tcp_mvp_plan_create.argtypes = [u32, u64, u32, u64p, u64p, f64p, i32, u64, ctypes.POINTER(vp)]
+        lib.tcp_mvp_plan_destroy.argtypes = [vp]
+        lib.tcp_mvp_plan_info.argtypes = [vp, ctypes.POINTER(TcpPlanInfo)]
+        lib.tcp_mvp_apply_into_host.argtypes = [vp, f64p, u64, f64p, u64, u64]
+        lib.tcp_mvp_apply_into_host_c64.argtypes = [vp, f32p, u64, f32p, u64]
+        lib.tcp_mvp_apply_into_device.argtypes = [vp, vp, vp, u64, u32, i32, vp]
+        lib.tcp_mvp_plan_device_status.argtypes = [vp]
+        lib.tcp_mvp_transition_count.argtypes = [vp, u64p]
+        lib.tcp_mvp_diagonal_device.argtypes = [vp, vp, u64, vp]
+        for name in EXPORTED_SYMBOLS:
+            if name not in ("tcp_last_error",):
+                getattr(lib, name).restype = i32
+        _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    lib = load_library()
+    buf = ctypes.create_string_buffer(1024)
+    lib.tcp_last_error(buf, len(buf))
+    return buf.value.decode("utf-8", "replace")
+
+
+class NativeDeviceError(RuntimeError):
+    """A CUDA runtime failure or an expired device-side wait."""
+
+    def __init__(self, message: str, status: int) -> None:
+        super().__init__(message)
+        self.status = status
+
+
+def raise_for_status(status: int) -> None:
+    """Map a C-ABI status to the reference's Python exception classes.
+
+    ``crates/tencirpauli-native/src/convert.rs:35-42``: MemoryLimit ->
+    MemoryError, Overflow -> OverflowError, every other PauliError ->
+    ValueError.  Device failures raise :class:`NativeDeviceError`; a failed
+    device allocation raises MemoryError.
+    """
+    if status == TCP_OK:
+        return
+    message = last_error()
+    if status == TCP_ERR_MEMORY_LIMIT or status == TCP_ERR_ALLOCATION:
+        raise MemoryError(message)
+    if status == TCP_ERR_OVERFLOW:
+        raise OverflowError(message)
+    if status in (TCP_ERR_CUDA, TCP_ERR_DEVICE_TIMEOUT, TCP_ERR_WRONG_DEVICE):
+        raise NativeDeviceError(message, status)
+    raise ValueError(message)
+
+
+def _ptr(array: np.ndarray, ctype: Any) -> Any:
+    return array.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def canonicalize(
+    nqubits: int, codes: np.ndarray, coefficients: np.ndarray
+) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Canonicalize code rows through ``tcp_pauli_canonicalize`` (no device needed)."""
+    lib = load_library()
+    count = int(coefficients.shape[0])
+    width = nqubits // 64 + (nqubits % 64 != 0)
+    codes = np.ascontiguousarray(codes, dtype=np.uint8).reshape(count, nqubits)
+    coeffs = np.ascontiguousarray(coefficients, dtype=np.complex128)
+    out_x = np.zeros((max(count, 1), width), dtype=np.uint64)
+    out_z = np.zeros((max(count, 1), width), dtype=np.uint64)
+    out_c = np.zeros(max(count, 1), dtype=np.complex128)
+    out_n = np.zeros(1, dtype=np.uint64)
+    bad = np.zeros(1, dtype=np.uint64)
+    status = lib.tcp_pauli_canonicalize(
+        nqubits,
+        count,
+        _ptr(codes, ctypes.c_uint8),
+        _ptr(coeffs.view(np.float64), ctypes.c_double),
+        _ptr(out_x, ctypes.c_uint64),
+        _ptr(out_z, ctypes.c_uint64),
+        _ptr(out_c.view(np.float64), ctypes.c_double),
+        _ptr(out_n, ctypes.c_uint64),
+        _ptr(bad, ctypes.c_uint64),
+    )
+    raise_for_status(status)
+    t = int(out_n[0])
+    return out_x[:t].copy(), out_z[:t].copy(), out_c[:t].copy()
+
+
+class NativeMvpPlan:
+    """Execution handle of one device plan (mirror of the PyO3 ``NativeMvpPlan``,
+    ``crates/tencirpauli-native/src/hamiltonian.rs:31-34,137-194``).
+
+    Exposes ``nqubits``, ``term_count``, ``transition_count``,
+    ``native_variant == "pauli"``, ``apply(state, max_bytes)`` and
+    ``apply_into(state, output, max_bytes)`` on host complex128 arrays, plus
+    device-resident entry points for torch CUDA tensors.
+    """
+
+    native_variant = "pauli"
+
+    def __init__(
+        self,
+        nqubits: int,
+        x_words: np.ndarray,
+        z_words: np.ndarray,
+        coefficients: np.ndarray,
+        storage: str = "lazy",
+        max_bytes: int = sys.maxsize,
+    ) -> None:
+        lib = load_library()
+        self._lib = lib
+        self._handle = ctypes.c_void_p(None)
+        if storage not in ("lazy", "eager"):
+            raise ValueError("invalid sector: storage must be either 'eager' or 'lazy'")
+        count = int(coefficients.shape[0])
+        width = nqubits // 64 + (nqubits % 64 != 0)
+        xw = np.ascontiguousarray(x_words, dtype=np.uint64).reshape(count * width)
+        zw = np.ascontiguousarray(z_words, dtype=np.uint64).reshape(count * width)
+        coeffs = np.ascontiguousarray(coefficients, dtype=np.complex128)
+        if count == 0:  # keep valid pointers for empty operators
+            xw = np.zeros(1, np.uint64)
+            zw = np.zeros(1, np.uint64)
+            coeffs = np.zeros(1, np.complex128)
+        handle = ctypes.c_void_p(None)
+        status = lib.tcp_mvp_plan_create(
+            nqubits,
+            count,
+            width,
+            _ptr(xw, ctypes.c_uint64),
+            _ptr(zw, ctypes.c_uint64),
+            _ptr(coeffs.view(np.float64), ctypes.c_double),
+            TCP_STORAGE_EAGER if storage == "eager" else TCP_STORAGE_LAZY,
+            min(int(max_bytes), U64_MAX),
+            ctypes.byref(handle),
+        )
+        raise_for_status(status)
+        self._handle = handle
+        info = TcpPlanInfo()
+        raise_for_status(lib.tcp_mvp_plan_info(handle, ctypes.byref(info)))
+        self._info = info
+        self.storage = storage
+
+    def __del__(self) -> None:
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value:
+            try:
+                self._lib.tcp_mvp_plan_destroy(handle)
+            except Exception:  # interpreter shutdown
+                pass
+            self._handle = ctypes.c_void_p(None)
+
+    # -- metadata ---------------------------------------------------------
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._handle
+
+    @property
+    def nqubits(self) -> int:
+        return int(self._info.nqubits)
+
+    @property
+    def dimension(self) -> int:
+        return int(self._info.dimension)
+
+    @property
+    def term_count(self) -> int:
+        return int(self._info.term_count)
+
+    @property
+    def group_count(self) -> int:
+        return int(self._info.group_count)
+
+    @property
+    def transition_count(self) -> Optional[int]:
+        value = int(self._info.transition_count)
+        return None if value < 0 else value
+
+    @property
+    def device(self) -> int:
+        return int(self._info.device)
+
+    @property
+    def info(self) -> TcpPlanInfo:
+        return self._info
+
+    # -- host apply (drop-in for MvpPlan::apply / apply_into) ---------------
+    def apply_into(self, state: np.ndarray, output: np.ndarray, max_bytes: int) -> None:
+        """``NativeMvpPlan.apply_into`` (hamiltonian.rs:176-193): strict buffers."""
+        for name, value in (("input", state), ("output", output)):
+            if not isinstance(value, np.ndarray):
+                raise TypeError("apply_into input and output must be NumPy arrays")
+            if value.dtype != np.complex128:
+                raise TypeError("apply_into input and output must have dtype complex128")
+            if value.ndim != 1:
+                raise ValueError(f"apply_into {name} must be one-dimensional")
+            if not value.flags.c_contiguous:
+                raise ValueError(f"apply_into {name} must be C-contiguous")
+        if not output.flags.writeable:
+            raise ValueError("apply_into output must be writable")
+        status = self._lib.tcp_mvp_apply_into_host(
+            self._handle,
+            _ptr(state.view(np.float64), ctypes.c_double),
+            state.shape[0],
+            _ptr(output.view(np.float64), ctypes.c_double),
+            output.shape[0],
+            min(int(max_bytes), U64_MAX),
+        )
+        raise_for_status(status)
+
+    def apply(self, state: np.ndarray, max_bytes: int) -> np.ndarray:
+        """``NativeMvpPlan.apply`` (hamiltonian.rs:160-174): owned complex128 output."""
+        values = np.ascontiguousarray(state, dtype=np.complex128)
+        if values.ndim != 1:
+            raise ValueError(f"state must be one-dimensional, got shape {values.shape}")
+        if values.shape[0] != self.dimension:
+            raise ValueError(
+                f"expected structure length {self.dimension}, got {values.shape[0]}"
+            )
+        out = np.empty(self.dimension, dtype=np.complex128)
+        self.apply_into(values, out, max_bytes)
+        return out
+
+    def apply_c64(self, state: np.ndarray) -> np.ndarray:
+        """Host complex64 apply (FP32 products, Kahan-compensated group sums)."""
+        values = np.ascontiguousarray(state, dtype=np.complex64)
+        out = np.empty(values.shape[0], dtype=np.complex64)
+        self.apply_c64_into(values, out)
+        return out
+
+    def apply_c64_into(self, state: np.ndarray, output: np.ndarray) -> None:
+        """complex64 host buffers, overwritten output (strict, like apply_into)."""
+        for value in (state, output):
+            if not isinstance(value, np.ndarray) or value.dtype != np.complex64:
+                raise TypeError("apply_c64_into input and output must be complex64 NumPy arrays")
+            if value.ndim != 1 or not value.flags.c_contiguous:
+                raise ValueError("apply_c64_into buffers must be one-dimensional and C-contiguous")
+        status = self._lib.tcp_mvp_apply_into_host_c64(
+            self._handle,
+            _ptr(state.view(np.float32), ctypes.c_float),
+            state.shape[0],
+            _ptr(output.view(np.float32), ctypes.c_float),
+            output.shape[0],
+        )
+        raise_for_status(status)
+
+    # -- device apply -----------------------------------------------------
+    def apply_device(self, x: Any, y: Any, stream: Any = None) -> None:
+        """Apply to torch CUDA tensors of shape (dim,) or (nrhs, dim).
+
+        complex128 tensors run the FP64 kernel, complex64 tensors the FP32
+        Kahan kernel.  Asynchronous on ``stream`` (default: torch's current
+        stream on the plan's device).
+        """
+        import torch
+
+        if not (isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor)):
+            raise TypeError("apply_device needs torch tensors")
+        if x.device.type != "cuda" or y.device.type != "cuda":
+            raise ValueError("apply_device needs CUDA tensors")
+        if x.dtype != y.dtype or x.dtype not in (torch.complex128, torch.complex64):
+            raise TypeError("apply_device tensors must both be complex128 or complex64")
+        if x.shape != y.shape or x.ndim not in (1, 2) or x.shape[-1] != self.dimension:
+            raise ValueError(f"apply_device tensors must have shape ({self.dimension},) or (nrhs, {self.dimension})")
+        if not (x.is_contiguous() and y.is_contiguous()):
+            raise ValueError("apply_device tensors must be contiguous")
+        nrhs = 1 if x.ndim == 1 else int(x.shape[0])
+        if stream is None:
+            stream = torch.cuda.current_stream(x.device)
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        dtype = TCP_DTYPE_C128 if x.dtype == torch.complex128 else TCP_DTYPE_C64
+        status = self._lib.tcp_mvp_apply_into_device(
+            self._handle,
+            ctypes.c_void_p(x.data_ptr()),
+            ctypes.c_void_p(y.data_ptr()),
+            self.dimension,
+            nrhs,
+            dtype,
+            ctypes.c_void_p(handle),
+        )
+        raise_for_status(status)
+
+    def diagonal_device(self, out: Any, stream: Any = None) -> None:
+        """Write H_ii (complex128, the x_mask == 0 group) into a CUDA tensor."""
+        import torch
+
+        if out.dtype != torch.complex128 or out.shape != (self.dimension,) or not out.is_contiguous():
+            raise ValueError("diagonal_device needs a contiguous complex128 tensor of length dim")
+        if stream is None:
+            stream = torch.cuda.current_stream(out.device)
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        raise_for_status(
+            self._lib.tcp_mvp_diagonal_device(
+                self._handle, ctypes.c_void_p(out.data_ptr()), self.dimension, ctypes.c_void_p(handle)
+            )
+        )
+
+    def device_status(self) -> None:
+        """Synchronise and raise if a kernel of this plan reported a device error."""
+        raise_for_status(self._lib.tcp_mvp_plan_device_status(self._handle))

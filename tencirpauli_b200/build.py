@@ -1,0 +1,68 @@
+"""Compile ``libtcpmvp.so`` in-tree for sm_100a with nvcc.
+
+The library is a plain C-ABI shared object (no torch or Python inside); it is
+written to ``tencirpauli_b200/_lib/libtcpmvp.so`` so that it travels with the
+source tree.  Run ``python -m tencirpauli_b200.build`` or call :func:`build`.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from typing import List
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+LIBPATH = os.path.join(LIBDIR, "libtcpmvp.so")
+SOURCES = ["tcp_plan.cpp", "tcp_mvp.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for candidate in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if candidate and os.path.exists(candidate):
+            return candidate
+    raise RuntimeError("nvcc not found")
+
+
+def _host_compiler() -> List[str]:
+    # nvcc needs a host g++ whose OpenMP/libstdc++ runtime exists on this image.
+    gxx = "/usr/bin/g++"
+    return ["-ccbin", gxx] if os.path.exists(gxx) else []
+
+
+def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    cmd = [
+        nvcc(),
+        *ARCH,
+        *_host_compiler(),
+        "-O3",
+        "-lineinfo",
+        "-std=c++17",
+        "-shared",
+        "-Xcompiler",
+        "-fPIC,-O3",
+        "--expt-relaxed-constexpr",
+        "-o",
+        LIBPATH + ".tmp",
+    ]
+    if ptxas_verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc failed:\n{proc.stdout}\n{proc.stderr}")
+    if ptxas_verbose or verbose:
+        sys.stdout.write(proc.stdout + proc.stderr)
+    os.replace(LIBPATH + ".tmp", LIBPATH)
+    return LIBPATH
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_verbose="-v" in sys.argv)

@@ -1,0 +1,715 @@
+// libtcpmvp.so -- sm_100a kernels and the C ABI of the matrix-free Pauli MVP.
+//
+// Kernels (all hand-written for sm_100a):
+//   k_tiled     tile-staged grouped MVP.  One CTA owns an output tile of
+//               2^S consecutive rows and keeps its accumulators in registers;
+//               for every outer pattern d ("step") the source tile
+//               (tile ^ d) is copied into shared memory by the TMA bulk-copy
+//               engine (cp.async.bulk + mbarrier, double-buffered), and every
+//               x-mask group of that step is applied from shared memory:
+//               D_m(c) = sum_{k in m} w_k (-1)^{popcount(z_k & c)} evaluated
+//               at the source column c = r ^ m, then y[r] += D_m(c) x[c].
+//               FP64 (complex128) and FP32-with-Kahan (complex64) variants.
+//   k_rowwise   one thread per row, direct gathers; for states smaller than
+//               one tile and for buffers the bulk-copy engine cannot address.
+//   k_transitions / k_diagonal   eager transition count and H_ii extraction.
+//
+// Reference semantics (paths inside the reference project):
+//   crates/tencir-pauli-core/src/hamiltonian.rs:204-270 (apply_into),
+//   :121-139 (eager diagonal), :166-179 (transition_count).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tcp_internal.h"
+
+using tcp::fail;
+
+namespace {
+
+constexpr int kLogThreads = 9;               // 512 threads per CTA
+constexpr int kThreads = 1 << kLogThreads;
+constexpr int kLogRowsC128 = 3;              // 8 rows per thread  -> 4096-row tile
+constexpr int kLogRowsC64 = 4;               // 16 rows per thread -> 8192-row tile
+constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
+constexpr uint32_t kTileBitsC64 = kLogThreads + kLogRowsC64;
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
+
+// Error bits written by kernels into the plan's device status word.
+constexpr int kErrTimeout = 1;
+
+struct DevSchedule {
+    const uint64_t *step_d;
+    const uint32_t *step_gbeg;
+    const uint32_t *g_min;
+    const uint32_t *g_tbeg;
+    const uint64_t *t_z;
+    const double2 *t_w;
+    const float2 *t_wf;
+    uint32_t nsteps;
+    uint32_t tile_bits;
+};
+
+// ------------------------------- PTX helpers -------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// 1-D bulk copy global -> shared through the TMA engine; completes tx bytes
+// on the mbarrier.  Both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait on an mbarrier phase: returns false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long start = global_ns();
+    for (uint32_t spin = 1;; ++spin) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((spin & 255u) == 0u && global_ns() - start > kWaitLimitNs) return false;
+    }
+}
+
+// ------------------------------ complex types ------------------------------
+template <typename R> struct Cx;
+template <> struct Cx<double> { using T = double2; };
+template <> struct Cx<float> { using T = float2; };
+
+template <typename R> __device__ __forceinline__ typename Cx<R>::T weight_of(const DevSchedule &s, uint32_t t);
+template <> __device__ __forceinline__ double2 weight_of<double>(const DevSchedule &s, uint32_t t) {
+    return __ldg(&s.t_w[t]);
+}
+template <> __device__ __forceinline__ float2 weight_of<float>(const DevSchedule &s, uint32_t t) {
+    return __ldg(&s.t_wf[t]);
+}
+
+// Accumulator of one output row: FP64 plain sum, FP32 Kahan-compensated sum
+// (one compensation term per component, carried across x-mask groups).
+template <typename R> struct Acc;
+template <> struct Acc<double> {
+    double re = 0.0, im = 0.0;
+    __device__ __forceinline__ void add_product(double dre, double dim, double2 v) {
+        re = fma(dre, v.x, re);
+        re = fma(-dim, v.y, re);
+        im = fma(dre, v.y, im);
+        im = fma(dim, v.x, im);
+    }
+    __device__ __forceinline__ double2 value() const { return make_double2(re, im); }
+};
+template <> struct Acc<float> {
+    float re = 0.f, im = 0.f, cre = 0.f, cim = 0.f;
+    __device__ __forceinline__ static void kahan(float &sum, float &comp, float term) {
+        float yv = term - comp;
+        float tv = __fadd_rn(sum, yv);
+        comp = __fsub_rn(__fsub_rn(tv, sum), yv);
+        sum = tv;
+    }
+    __device__ __forceinline__ void add_product(float dre, float dim, float2 v) {
+        float pre = __fmaf_rn(dre, v.x, -dim * v.y);
+        float pim = __fmaf_rn(dre, v.y, dim * v.x);
+        kahan(re, cre, pre);
+        kahan(im, cim, pim);
+    }
+    __device__ __forceinline__ float2 value() const { return make_float2(re, im); }
+};
+
+// --------------------------------- kernels ---------------------------------
+// Tile-staged grouped MVP (see file header).  Grid: one CTA per output tile.
+template <int LOGE, typename R>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_tiled(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
+            int *__restrict__ err) {
+    using C = typename Cx<R>::T;
+    constexpr int E = 1 << LOGE;
+    constexpr int S = kLogThreads + LOGE;
+    constexpr uint32_t TILE = 1u << S;
+    constexpr uint32_t BYTES = TILE * sizeof(C);
+    constexpr int CH = 4;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    C *buf[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + TILE};
+    __shared__ __align__(8) uint64_t bars[2];
+
+    const uint32_t tid = threadIdx.x;
+    const uint64_t tile = blockIdx.x;
+    const uint32_t nsteps = s.nsteps;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0 && nsteps > 0) {
+        mbar_arrive_expect_tx(&bars[0], BYTES);
+        bulk_copy_g2s(buf[0], x + ((tile ^ s.step_d[0]) << S), BYTES, &bars[0]);
+    }
+
+    Acc<R> acc[E];
+    for (uint32_t st = 0; st < nsteps; ++st) {
+        const uint32_t b = st & 1u;
+        bool ok = mbar_wait_bounded(&bars[b], (st >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(err, kErrTimeout);
+            return;
+        }
+        // Every thread has finished step st-1, so the other buffer is free.
+        if (tid == 0 && st + 1 < nsteps) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bars[b ^ 1u], BYTES);
+            bulk_copy_g2s(buf[b ^ 1u], x + ((tile ^ s.step_d[st + 1]) << S), BYTES, &bars[b ^ 1u]);
+        }
+        const C *xs = buf[b];
+        const uint64_t src_base = (tile ^ s.step_d[st]) << S;
+        const uint32_t gb = s.step_gbeg[st], ge = s.step_gbeg[st + 1];
+        for (uint32_t g = gb; g < ge; ++g) {
+            const uint32_t m = __ldg(&s.g_min[g]);
+            const uint32_t tl = tid ^ (m & (kThreads - 1));
+            const uint32_t jh = m >> kLogThreads;
+            const uint32_t tb = __ldg(&s.g_tbeg[g]), te = __ldg(&s.g_tbeg[g + 1]);
+            // Rows are processed CH at a time to bound register use.
+#pragma unroll
+            for (int j0 = 0; j0 < E; j0 += CH) {
+                uint32_t col[CH];
+                C xv[CH];
+                R dre[CH], dim[CH];
+#pragma unroll
+                for (int jj = 0; jj < CH; ++jj) {
+                    col[jj] = tl | ((static_cast<uint32_t>(j0 + jj) ^ jh) << kLogThreads);
+                    xv[jj] = xs[col[jj]];
+                    dre[jj] = dim[jj] = R(0);
+                }
+                for (uint32_t t = tb; t < te; ++t) {
+                    const uint64_t z = __ldg(&s.t_z[t]);
+                    const C w = weight_of<R>(s, t);
+                    const uint32_t ph = static_cast<uint32_t>(__popcll(z & src_base));
+                    const uint32_t zl = static_cast<uint32_t>(z) & (TILE - 1);
+#pragma unroll
+                    for (int jj = 0; jj < CH; ++jj) {
+                        const bool neg = (__popc(zl & col[jj]) + ph) & 1u;
+                        dre[jj] = dre[jj] + (neg ? -w.x : w.x);
+                        dim[jj] = dim[jj] + (neg ? -w.y : w.y);
+                    }
+                }
+#pragma unroll
+                for (int jj = 0; jj < CH; ++jj) acc[j0 + jj].add_product(dre[jj], dim[jj], xv[jj]);
+            }
+        }
+    }
+    C *yt = y + (tile << S);
+#pragma unroll
+    for (int j = 0; j < E; ++j) yt[tid + (j << kLogThreads)] = acc[j].value();
+}
+
+// One thread per row; gathers straight from global memory.
+template <typename R>
+__global__ void k_rowwise(DevSchedule s, const typename Cx<R>::T *__restrict__ x,
+                          typename Cx<R>::T *__restrict__ y, uint64_t dim) {
+    using C = typename Cx<R>::T;
+    const uint32_t S = s.tile_bits;
+    for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; r < dim;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        Acc<R> acc;
+        for (uint32_t st = 0; st < s.nsteps; ++st) {
+            const uint64_t outer = s.step_d[st] << S;
+            for (uint32_t g = s.step_gbeg[st]; g < s.step_gbeg[st + 1]; ++g) {
+                const uint64_t c = r ^ (outer | s.g_min[g]);
+                const C v = x[c];
+                R dre = R(0), dimv = R(0);
+                for (uint32_t t = s.g_tbeg[g]; t < s.g_tbeg[g + 1]; ++t) {
+                    const C w = weight_of<R>(s, t);
+                    const bool neg = __popcll(s.t_z[t] & c) & 1;
+                    dre = dre + (neg ? -w.x : w.x);
+                    dimv = dimv + (neg ? -w.y : w.y);
+                }
+                acc.add_product(dre, dimv, v);
+            }
+        }
+        y[r] = acc.value();
+    }
+}
+
+// Eager transition count: nonzero D_m[c] over all groups m and columns c, with
+// D summed in canonical term order exactly as hamiltonian.rs:125-133.
+__global__ void k_transitions(DevSchedule s, uint32_t ngroups, uint64_t dim, unsigned long long *count) {
+    unsigned long long local = 0;
+    const uint64_t total = static_cast<uint64_t>(ngroups) * dim;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t g = static_cast<uint32_t>(i / dim);
+        const uint64_t c = i % dim;
+        double re = 0.0, im = 0.0;
+        for (uint32_t t = s.g_tbeg[g]; t < s.g_tbeg[g + 1]; ++t) {
+            const double2 w = s.t_w[t];
+            const bool neg = __popcll(s.t_z[t] & c) & 1;
+            re = re + (neg ? -w.x : w.x);
+            im = im + (neg ? -w.y : w.y);
+        }
+        local += (re != 0.0 || im != 0.0);
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+// H_ii: the x_mask == 0 group's diagonal (zero when the operator has none).
+__global__ void k_diagonal(DevSchedule s, uint32_t gzero, uint64_t dim, double2 *__restrict__ out) {
+    for (uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; c < dim;
+         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        double re = 0.0, im = 0.0;
+        if (gzero != 0xffffffffu) {
+            for (uint32_t t = s.g_tbeg[gzero]; t < s.g_tbeg[gzero + 1]; ++t) {
+                const double2 w = s.t_w[t];
+                const bool neg = __popcll(s.t_z[t] & c) & 1;
+                re = re + (neg ? -w.x : w.x);
+                im = im + (neg ? -w.y : w.y);
+            }
+        }
+        out[c] = make_double2(re, im);
+    }
+}
+
+// --------------------------------- host side --------------------------------
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(TCP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+cudaError_t dev_malloc(void **p, size_t bytes) {
+    if (tcp::injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
+struct DeviceSchedule {
+    tcp::Schedule host;
+    DevSchedule dev{};
+};
+
+struct Workspace {
+    void *x = nullptr;
+    void *y = nullptr;
+    size_t bytes = 0;
+};
+
+int g_num_sms = 0;
+
+}  // namespace
+
+struct tcp_mvp_plan {
+    uint32_t nqubits = 0;
+    uint32_t word_count = 0;
+    uint64_t dim = 0;
+    int storage = 0;
+    int device = 0;
+    int64_t transitions = -1;
+    std::vector<tcp::MatrixTerm> terms;
+    uint64_t group_count = 0;
+    DeviceSchedule c128;
+    DeviceSchedule c64;
+    void *dev_block = nullptr;
+    size_t dev_bytes = 0;
+    int *d_err = nullptr;
+    mutable std::mutex ws_mutex;
+    mutable std::vector<Workspace> ws_free;
+    mutable std::vector<Workspace> ws_all;
+};
+
+namespace {
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Lay both schedules out in one device allocation.
+int upload(tcp_mvp_plan *p) {
+    struct Piece {
+        const void *src;
+        size_t bytes;
+        const void **dst;
+    };
+    std::vector<Piece> pieces;
+    auto add = [&](const void *src, size_t bytes, const void **dst) { pieces.push_back({src, bytes, dst}); };
+    for (DeviceSchedule *ds : {&p->c128, &p->c64}) {
+        tcp::Schedule &h = ds->host;
+        add(h.step_d.data(), h.step_d.size() * 8, reinterpret_cast<const void **>(&ds->dev.step_d));
+        add(h.step_gbeg.data(), h.step_gbeg.size() * 4, reinterpret_cast<const void **>(&ds->dev.step_gbeg));
+        add(h.g_min.data(), h.g_min.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_min));
+        add(h.g_tbeg.data(), h.g_tbeg.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_tbeg));
+        add(h.t_z.data(), h.t_z.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_z));
+        add(h.t_w.data(), h.t_w.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_w));
+        add(h.t_wf.data(), h.t_wf.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wf));
+        ds->dev.nsteps = static_cast<uint32_t>(h.step_d.size());
+        ds->dev.tile_bits = h.tile_bits;
+    }
+    size_t total = 256;  // error word first
+    for (auto &pc : pieces) total = align_up(total, 256) + std::max<size_t>(pc.bytes, 16);
+    void *block = nullptr;
+    cudaError_t e = dev_malloc(&block, total);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TCP_ERR_ALLOCATION, std::string("device allocation of the plan failed: ") + cudaGetErrorString(e));
+    }
+    std::vector<unsigned char> staging(total, 0);
+    size_t off = 256;
+    for (auto &pc : pieces) {
+        off = align_up(off, 256);
+        if (pc.bytes) std::memcpy(staging.data() + off, pc.src, pc.bytes);
+        *pc.dst = static_cast<unsigned char *>(block) + off;
+        off += std::max<size_t>(pc.bytes, 16);
+    }
+    e = cudaMemcpy(block, staging.data(), total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(block);
+        return cuda_fail(e, "plan upload");
+    }
+    p->dev_block = block;
+    p->dev_bytes = total;
+    p->d_err = static_cast<int *>(block);
+    return TCP_OK;
+}
+
+int check_plan(const tcp_mvp_plan *plan) {
+    if (plan == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "plan is null");
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev != plan->device) {
+        return fail(TCP_ERR_WRONG_DEVICE, "plan lives on device " + std::to_string(plan->device) +
+                                              " but the current device is " + std::to_string(dev));
+    }
+    return TCP_OK;
+}
+
+int length_error(uint64_t expected, uint64_t actual) {
+    return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH,
+                "expected structure length " + std::to_string(expected) + ", got " + std::to_string(actual));
+}
+
+bool overlaps(const void *a, const void *b, size_t bytes) {
+    auto pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    return pa < pb + bytes && pb < pa + bytes;
+}
+
+template <int LOGE, typename R> int set_smem_attr() {
+    constexpr size_t bytes = 2 * (size_t(1) << (kLogThreads + LOGE)) * sizeof(typename Cx<R>::T);
+    cudaError_t e = cudaFuncSetAttribute(k_tiled<LOGE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "cudaFuncSetAttribute");
+}
+
+// Launch one right-hand side.
+template <typename R>
+int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t stream) {
+    using C = typename Cx<R>::T;
+    constexpr bool is64 = sizeof(R) == 8;
+    constexpr int LOGE = is64 ? kLogRowsC128 : kLogRowsC64;
+    const DeviceSchedule &ds = is64 ? p->c128 : p->c64;
+    const uint32_t S = kLogThreads + LOGE;
+    const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
+    if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
+        // The shared-memory opt-in is a per-device function attribute.
+        static std::mutex attr_mutex;
+        static bool attr_done[64] = {};
+        {
+            std::lock_guard<std::mutex> lock(attr_mutex);
+            if (p->device < 64 && !attr_done[p->device]) {
+                int attr_status = set_smem_attr<LOGE, R>();
+                if (attr_status != TCP_OK) return attr_status;
+                attr_done[p->device] = true;
+            }
+        }
+        const uint64_t tiles = p->dim >> S;
+        const size_t smem = 2 * (size_t(1) << S) * sizeof(C);
+        k_tiled<LOGE, R><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
+            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err);
+    } else {
+        const int threads = 256;
+        uint64_t blocks = (p->dim + threads - 1) / threads;
+        blocks = std::min<uint64_t>(blocks, 1u << 20);
+        k_rowwise<R><<<static_cast<unsigned>(blocks), threads, 0, stream>>>(
+            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->dim);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "MVP kernel launch");
+}
+
+int read_device_status(const tcp_mvp_plan *p) {
+    int h = 0;
+    cudaError_t e = cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "reading device status");
+    if (h != 0) {
+        int zero = 0;
+        cudaMemcpy(p->d_err, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        if (h & kErrTimeout) return fail(TCP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+    }
+    return TCP_OK;
+}
+
+template <typename R>
+int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *result, uint64_t result_len) {
+    int st = check_plan(plan);
+    if (st) return st;
+    if (state_len != plan->dim) return length_error(plan->dim, state_len);
+    if (result_len != plan->dim) return length_error(plan->dim, result_len);
+    if (state == nullptr || result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t bytes = plan->dim * 2 * sizeof(R);
+    if (overlaps(state, result, bytes)) return fail(TCP_ERR_INVALID_ARGUMENT, "input and output must not overlap");
+    Workspace ws;
+    {
+        std::lock_guard<std::mutex> lock(plan->ws_mutex);
+        for (size_t i = 0; i < plan->ws_free.size(); ++i) {
+            if (plan->ws_free[i].bytes >= bytes) {
+                ws = plan->ws_free[i];
+                plan->ws_free.erase(plan->ws_free.begin() + static_cast<long>(i));
+                break;
+            }
+        }
+    }
+    if (ws.x == nullptr) {
+        cudaError_t e1 = dev_malloc(&ws.x, bytes);
+        cudaError_t e2 = e1 == cudaSuccess ? dev_malloc(&ws.y, bytes) : e1;
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            cudaGetLastError();
+            if (ws.x) cudaFree(ws.x);
+            return fail(TCP_ERR_ALLOCATION, "device allocation of the apply workspace failed");
+        }
+        ws.bytes = bytes;
+        std::lock_guard<std::mutex> lock(plan->ws_mutex);
+        plan->ws_all.push_back(ws);
+    }
+    cudaStream_t stream = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    int status = TCP_OK;
+    if (e != cudaSuccess) status = cuda_fail(e, "cudaStreamCreate");
+    if (!status) {
+        e = cudaMemcpyAsync(ws.x, state, bytes, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
+    }
+    if (!status) status = launch_one<R>(plan, ws.x, ws.y, stream);
+    if (!status) {
+        e = cudaMemcpyAsync(result, ws.y, bytes, cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+    }
+    if (stream) {
+        e = cudaStreamSynchronize(stream);
+        if (!status && e != cudaSuccess) status = cuda_fail(e, "stream synchronize");
+        cudaStreamDestroy(stream);
+    }
+    if (!status) status = read_device_status(plan);
+    {
+        std::lock_guard<std::mutex> lock(plan->ws_mutex);
+        plan->ws_free.push_back(ws);
+    }
+    return status;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32_t word_count,
+                                   const uint64_t *x_words, const uint64_t *z_words, const double *coefficients,
+                                   int storage, uint64_t max_bytes, tcp_mvp_plan **out_plan) {
+    if (out_plan == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "out_plan is null");
+    *out_plan = nullptr;
+    if (storage != TCP_STORAGE_LAZY && storage != TCP_STORAGE_EAGER) {
+        return fail(TCP_ERR_INVALID_SECTOR, "invalid sector: storage must be either 'eager' or 'lazy'");
+    }
+    if (term_count > 0 && (x_words == nullptr || z_words == nullptr || coefficients == nullptr)) {
+        return fail(TCP_ERR_INVALID_ARGUMENT, "null term arrays");
+    }
+    if (term_count > 0xffffffffull) return fail(TCP_ERR_OVERFLOW, "integer overflow while counting plan terms");
+    std::unique_ptr<tcp_mvp_plan> p(new tcp_mvp_plan());
+    int st = tcp::compile_terms(nqubits, term_count, word_count, x_words, z_words, coefficients, p->terms);
+    if (st) return st;
+    p->nqubits = nqubits;
+    p->word_count = word_count;
+    p->dim = 1ull << nqubits;
+    p->storage = storage;
+    p->group_count = tcp::distinct_x_masks(p->terms);
+    if (storage == TCP_STORAGE_EAGER) {
+        // from_operator_reusable budget (hamiltonian.rs:84-119): G*dim*16
+        // diagonal bytes (+ 2 * T * 32 term bytes + G * 32 group headers).
+        unsigned __int128 diag = static_cast<unsigned __int128>(p->group_count) * p->dim * 16u;
+        unsigned __int128 term_bytes = static_cast<unsigned __int128>(term_count) * 32u;
+        if (diag >> 64) return fail(TCP_ERR_OVERFLOW, "integer overflow while estimating reusable MVP plan memory");
+        if (term_bytes > max_bytes) {
+            return fail(TCP_ERR_MEMORY_LIMIT, "requested " + std::to_string(static_cast<uint64_t>(term_bytes)) +
+                                                  " bytes exceeds memory limit " + std::to_string(max_bytes));
+        }
+        unsigned __int128 construction = diag + 2 * term_bytes + static_cast<unsigned __int128>(p->group_count) * 32u;
+        if (construction > max_bytes) {
+            std::string req = construction >> 64 ? std::string("more than 2^64")
+                                                  : std::to_string(static_cast<uint64_t>(construction));
+            return fail(TCP_ERR_MEMORY_LIMIT, "requested " + req + " bytes exceeds memory limit " + std::to_string(max_bytes));
+        }
+    }
+    cudaError_t e = cudaGetDevice(&p->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (g_num_sms == 0) cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, p->device);
+    p->c128.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128);
+    p->c64.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC64);
+    st = upload(p.get());
+    if (st) return st;
+    if (storage == TCP_STORAGE_EAGER) {
+        uint64_t count = 0;
+        st = tcp_mvp_transition_count(p.get(), &count);
+        if (st) {
+            cudaFree(p->dev_block);
+            return st;
+        }
+        p->transitions = static_cast<int64_t>(count);
+    }
+    *out_plan = p.release();
+    return TCP_OK;
+}
+
+extern "C" int tcp_mvp_plan_destroy(tcp_mvp_plan *plan) {
+    if (plan == nullptr) return TCP_OK;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != plan->device) cudaSetDevice(plan->device);
+    for (auto &w : plan->ws_all) {
+        cudaFree(w.x);
+        cudaFree(w.y);
+    }
+    if (plan->dev_block) cudaFree(plan->dev_block);
+    if (prev >= 0 && prev != plan->device) cudaSetDevice(prev);
+    delete plan;
+    return TCP_OK;
+}
+
+extern "C" int tcp_mvp_plan_info(const tcp_mvp_plan *plan, tcp_mvp_plan_info_t *info) {
+    if (plan == nullptr || info == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null argument");
+    info->nqubits = plan->nqubits;
+    info->word_count = plan->word_count;
+    info->dimension = plan->dim;
+    info->term_count = plan->terms.size();
+    info->group_count = plan->group_count;
+    info->storage = plan->storage;
+    info->device = plan->device;
+    info->transition_count = plan->transitions;
+    info->device_bytes = plan->dev_bytes;
+    info->tile_bits_c128 = plan->c128.host.tile_bits;
+    info->tile_bits_c64 = plan->c64.host.tile_bits;
+    info->steps_c128 = plan->c128.host.step_d.size();
+    info->steps_c64 = plan->c64.host.step_d.size();
+    return TCP_OK;
+}
+
+extern "C" int tcp_mvp_apply_into_host(const tcp_mvp_plan *plan, const double *state, uint64_t state_len,
+                                       double *result, uint64_t result_len, uint64_t max_bytes) {
+    (void)max_bytes;  // advisory, ignored by the reference apply (hamiltonian.rs:223)
+    return apply_host<double>(plan, state, state_len, result, result_len);
+}
+
+extern "C" int tcp_mvp_apply_into_host_c64(const tcp_mvp_plan *plan, const float *state, uint64_t state_len,
+                                           float *result, uint64_t result_len) {
+    return apply_host<float>(plan, state, state_len, result, result_len);
+}
+
+extern "C" int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
+                                         uint64_t len, uint32_t nrhs, int dtype, void *stream) {
+    int st = check_plan(plan);
+    if (st) return st;
+    if (len != plan->dim) return length_error(plan->dim, len);
+    if (dtype != TCP_DTYPE_C128 && dtype != TCP_DTYPE_C64) return fail(TCP_ERR_INVALID_ARGUMENT, "unknown dtype");
+    if (nrhs == 0) return TCP_OK;
+    if (d_state == nullptr || d_result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    const size_t elem = dtype == TCP_DTYPE_C128 ? 16 : 8;
+    const size_t bytes = static_cast<size_t>(len) * elem * nrhs;
+    if (overlaps(d_state, d_result, bytes)) return fail(TCP_ERR_INVALID_ARGUMENT, "input and output must not overlap");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (uint32_t v = 0; v < nrhs; ++v) {
+        const void *x = static_cast<const unsigned char *>(d_state) + static_cast<size_t>(v) * len * elem;
+        void *y = static_cast<unsigned char *>(d_result) + static_cast<size_t>(v) * len * elem;
+        st = dtype == TCP_DTYPE_C128 ? launch_one<double>(plan, x, y, s) : launch_one<float>(plan, x, y, s);
+        if (st) return st;
+    }
+    return TCP_OK;
+}
+
+extern "C" int tcp_mvp_plan_device_status(const tcp_mvp_plan *plan) {
+    int st = check_plan(plan);
+    if (st) return st;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+    return read_device_status(plan);
+}
+
+extern "C" int tcp_mvp_transition_count(const tcp_mvp_plan *plan, uint64_t *out_count) {
+    int st = check_plan(plan);
+    if (st) return st;
+    if (out_count == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "out_count is null");
+    unsigned long long *d_count = nullptr;
+    cudaError_t e = dev_malloc(reinterpret_cast<void **>(&d_count), sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TCP_ERR_ALLOCATION, "device allocation of the transition counter failed");
+    }
+    cudaMemset(d_count, 0, sizeof(unsigned long long));
+    const uint32_t ngroups = static_cast<uint32_t>(plan->c128.host.g_min.size());
+    const uint64_t total = static_cast<uint64_t>(ngroups) * plan->dim;
+    if (total > 0) {
+        const int threads = 256;
+        uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 148ull * 64);
+        k_transitions<<<static_cast<unsigned>(blocks), threads>>>(plan->c128.dev, ngroups, plan->dim, d_count);
+    }
+    unsigned long long h = 0;
+    e = cudaMemcpy(&h, d_count, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d_count);
+    if (e != cudaSuccess) return cuda_fail(e, "transition count");
+    *out_count = h;
+    return TCP_OK;
+}
+
+extern "C" int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, uint64_t len, void *stream) {
+    int st = check_plan(plan);
+    if (st) return st;
+    if (len != plan->dim) return length_error(plan->dim, len);
+    if (d_diag == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    const tcp::Schedule &h = plan->c128.host;
+    uint32_t gzero = 0xffffffffu;
+    if (!h.step_d.empty() && h.step_d[0] == 0 && !h.g_min.empty() && h.g_min[0] == 0) gzero = 0;
+    const int threads = 256;
+    uint64_t blocks = std::min<uint64_t>((plan->dim + threads - 1) / threads, 1u << 20);
+    k_diagonal<<<static_cast<unsigned>(blocks), threads, 0, static_cast<cudaStream_t>(stream)>>>(
+        plan->c128.dev, gzero, plan->dim, static_cast<double2 *>(d_diag));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "diagonal kernel launch");
+}

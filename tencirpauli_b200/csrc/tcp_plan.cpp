@@ -1,0 +1,246 @@
+// Host side of libtcpmvp.so: error slot, canonicalization, term compilation and
+// the tile schedule.  Pure C++ (no CUDA); compiled by nvcc with the kernels.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <numeric>
+
+#include "tcp_internal.h"
+
+namespace tcp {
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<long long> g_alloc_count{0};
+}  // namespace
+
+void set_error(const std::string &message) { g_last_error = message; }
+
+int fail(int status, const std::string &message) {
+    g_last_error = message;
+    return status;
+}
+
+bool injected_alloc_failure() {
+    const char *env = std::getenv("TCP_FAIL_ALLOC_AFTER");
+    if (env == nullptr || *env == '\0') return false;
+    long long limit = std::atoll(env);
+    long long index = g_alloc_count.fetch_add(1);
+    return index >= limit;
+}
+
+static inline uint32_t packed_word_count(uint32_t nqubits) { return nqubits / 64 + (nqubits % 64 != 0); }
+
+int compile_terms(uint32_t nqubits, uint64_t count, uint32_t word_count, const uint64_t *x_words,
+                  const uint64_t *z_words, const double *coefficients, std::vector<MatrixTerm> &out) {
+    // pauli_action.rs:38-55 -- word-length and dimension checks
+    uint32_t expected = packed_word_count(nqubits);
+    if (word_count != expected) {
+        return fail(TCP_ERR_INVALID_WORD_LENGTH, "expected " + std::to_string(expected) +
+                                                     " packed words, got " + std::to_string(word_count));
+    }
+    if (nqubits >= 64) return fail(TCP_ERR_OVERFLOW, "integer overflow while computing dense statevector dimension");
+    out.clear();
+    out.reserve(count);
+    // word.rs:81-85: bits above nqubits in the final word are masked off
+    uint64_t tail = (nqubits % 64) ? ((1ull << (nqubits % 64)) - 1) : ~0ull;
+    for (uint64_t t = 0; t < count; ++t) {
+        double re = coefficients[2 * t], im = coefficients[2 * t + 1];
+        if (!std::isfinite(re) || !std::isfinite(im)) {
+            return fail(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite");
+        }
+        uint64_t xm = 0, zm = 0;
+        uint32_t ny = 0;
+        for (uint32_t q = 0; q < nqubits; ++q) {
+            uint64_t packed = 1ull << (q % 64);
+            uint64_t xw = x_words[t * word_count + q / 64];
+            uint64_t zw = z_words[t * word_count + q / 64];
+            if (q / 64 == word_count - 1) {
+                xw &= tail;
+                zw &= tail;
+            }
+            bool x = (xw & packed) != 0, z = (zw & packed) != 0;
+            uint64_t bit = 1ull << (nqubits - 1 - q);
+            if (x) xm |= bit;
+            if (z) zm |= bit;
+            if (x && z) ++ny;
+        }
+        // y_phase = i^{#Y mod 4}; weighted = coefficient * y_phase with the
+        // textbook complex product (num-complex): (a c - b d, a d + b c).
+        double pr = 0.0, pi = 0.0;
+        switch (ny % 4) {
+        case 0: pr = 1.0; break;
+        case 1: pi = 1.0; break;
+        case 2: pr = -1.0; break;
+        default: pi = -1.0; break;
+        }
+        MatrixTerm mt;
+        mt.x_mask = xm;
+        mt.z_mask = zm;
+        volatile double ac = re * pr, bd = im * pi, ad = re * pi, bc = im * pr;  // no contraction
+        mt.w_re = ac - bd;
+        mt.w_im = ad + bc;
+        out.push_back(mt);
+    }
+    return TCP_OK;
+}
+
+uint64_t distinct_x_masks(const std::vector<MatrixTerm> &terms) {
+    std::vector<uint64_t> m;
+    m.reserve(terms.size());
+    for (auto &t : terms) m.push_back(t.x_mask);
+    std::sort(m.begin(), m.end());
+    return static_cast<uint64_t>(std::unique(m.begin(), m.end()) - m.begin());
+}
+
+Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits) {
+    Schedule s;
+    s.tile_bits = std::min(tile_bits, nqubits);
+    const uint32_t S = s.tile_bits;
+    const uint64_t inner = (S >= 64) ? ~0ull : ((1ull << S) - 1);
+    // (outer, inner, canonical index): a stable order that keeps canonical
+    // term order inside every x-mask group.
+    std::vector<uint64_t> order(terms.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) {
+        uint64_t da = terms[a].x_mask >> S, db = terms[b].x_mask >> S;
+        if (da != db) return da < db;
+        return (terms[a].x_mask & inner) < (terms[b].x_mask & inner);
+    });
+    s.step_gbeg.push_back(0);
+    s.g_tbeg.push_back(0);
+    for (size_t i = 0; i < order.size(); ++i) {
+        const MatrixTerm &t = terms[order[i]];
+        uint64_t d = t.x_mask >> S;
+        uint32_t m = static_cast<uint32_t>(t.x_mask & inner);
+        bool new_step = s.step_d.empty() || s.step_d.back() != d;
+        bool new_group = new_step || s.g_min.back() != m;
+        if (new_group && !s.g_min.empty()) s.g_tbeg.push_back(static_cast<uint32_t>(s.t_z.size()));
+        if (new_step) {
+            if (!s.step_d.empty()) s.step_gbeg.push_back(static_cast<uint32_t>(s.g_min.size()));
+            s.step_d.push_back(d);
+        }
+        if (new_group) s.g_min.push_back(m);
+        s.t_z.push_back(t.z_mask);
+        s.t_w.push_back(t.w_re);
+        s.t_w.push_back(t.w_im);
+        s.t_wf.push_back(static_cast<float>(t.w_re));
+        s.t_wf.push_back(static_cast<float>(t.w_im));
+    }
+    if (!s.g_min.empty()) {
+        s.g_tbeg.push_back(static_cast<uint32_t>(s.t_z.size()));
+        s.step_gbeg.push_back(static_cast<uint32_t>(s.g_min.size()));
+    } else {
+        s.g_tbeg.assign(1, 0);
+        s.step_gbeg.assign(1, 0);
+    }
+    return s;
+}
+
+}  // namespace tcp
+
+// ---------------------------------------------------------------------------
+// C ABI: canonicalization (operator.rs:117-155)
+// ---------------------------------------------------------------------------
+namespace {
+inline uint8_t code_at(const uint64_t *xw, const uint64_t *zw, uint32_t q) {
+    uint64_t x = (xw[q / 64] >> (q % 64)) & 1u, z = (zw[q / 64] >> (q % 64)) & 1u;
+    return x ? (z ? 2 : 1) : (z ? 3 : 0);
+}
+inline uint64_t bits_of(double v) {
+    uint64_t b;
+    std::memcpy(&b, &v, sizeof b);
+    return b;
+}
+}  // namespace
+
+extern "C" int tcp_pauli_canonicalize(uint32_t nqubits, uint64_t count, const uint8_t *codes,
+                                      const double *coefficients, uint64_t *out_x, uint64_t *out_z,
+                                      double *out_coefficients, uint64_t *out_count, uint64_t *bad_index) {
+    using namespace tcp;
+    if (out_count == nullptr || (count > 0 && (coefficients == nullptr || out_coefficients == nullptr ||
+                                               out_x == nullptr || out_z == nullptr ||
+                                               (nqubits > 0 && codes == nullptr)))) {
+        return fail(TCP_ERR_INVALID_ARGUMENT, "null pointer argument");
+    }
+    const uint32_t w = packed_word_count(nqubits);
+    // Validation in input order, coefficient before codes (operator.rs:130-136).
+    for (uint64_t t = 0; t < count; ++t) {
+        if (!std::isfinite(coefficients[2 * t]) || !std::isfinite(coefficients[2 * t + 1])) {
+            if (bad_index) *bad_index = t;
+            return fail(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite");
+        }
+        for (uint32_t q = 0; q < nqubits; ++q) {
+            uint8_t c = codes[t * nqubits + q];
+            if (c > 3) {
+                if (bad_index) *bad_index = q;
+                return fail(TCP_ERR_INVALID_CODE,
+                            "invalid Pauli code " + std::to_string(c) + " at index " + std::to_string(q) + "; expected 0..=3");
+            }
+        }
+    }
+    std::vector<uint64_t> xw(count * w + 1, 0), zw(count * w + 1, 0);
+    for (uint64_t t = 0; t < count; ++t) {
+        for (uint32_t q = 0; q < nqubits; ++q) {
+            uint8_t c = codes[t * nqubits + q];
+            uint64_t x = (c == 1 || c == 2), z = (c == 2 || c == 3);
+            xw[t * w + q / 64] |= x << (q % 64);
+            zw[t * w + q / 64] |= z << (q % 64);
+        }
+    }
+    auto word_less = [&](uint64_t a, uint64_t b) -> int {
+        for (uint32_t q = 0; q < nqubits; ++q) {
+            uint8_t ca = code_at(&xw[a * w], &zw[a * w], q), cb = code_at(&xw[b * w], &zw[b * w], q);
+            if (ca != cb) return ca < cb ? -1 : 1;
+        }
+        return 0;
+    };
+    std::vector<uint64_t> idx(count);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+        int r = word_less(a, b);
+        if (r) return r < 0;
+        uint64_t ar = bits_of(coefficients[2 * a]), br = bits_of(coefficients[2 * b]);
+        if (ar != br) return ar < br;
+        uint64_t ai = bits_of(coefficients[2 * a + 1]), bi = bits_of(coefficients[2 * b + 1]);
+        if (ai != bi) return ai < bi;
+        return a < b;
+    });
+    uint64_t out = 0;
+    for (uint64_t i = 0; i < count;) {
+        uint64_t j = i;
+        double sr = 0.0, si = 0.0;
+        while (j < count && word_less(idx[i], idx[j]) == 0) {
+            sr = sr + coefficients[2 * idx[j]];
+            si = si + coefficients[2 * idx[j] + 1];
+            ++j;
+        }
+        if (!(sr == 0.0 && si == 0.0)) {
+            for (uint32_t k = 0; k < w; ++k) {
+                out_x[out * w + k] = xw[idx[i] * w + k];
+                out_z[out * w + k] = zw[idx[i] * w + k];
+            }
+            out_coefficients[2 * out] = sr;
+            out_coefficients[2 * out + 1] = si;
+            ++out;
+        }
+        i = j;
+    }
+    *out_count = out;
+    return TCP_OK;
+}
+
+extern "C" size_t tcp_last_error(char *buffer, size_t capacity) {
+    const std::string &m = tcp::g_last_error;
+    if (buffer != nullptr && capacity > 0) {
+        size_t n = std::min(capacity - 1, m.size());
+        std::memcpy(buffer, m.data(), n);
+        buffer[n] = '\0';
+    }
+    return m.size();
+}
+
+extern "C" int tcp_abi_version(void) { return TCP_ABI_VERSION; }

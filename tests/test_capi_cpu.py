@@ -1,0 +1,133 @@
+"""CPU-only checks of the C-ABI library: it loads, exports every declared
+symbol, and its host-side entry points (canonicalization, plan-budget errors)
+behave as the reference's.  No kernel is launched here."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden
+from oracle import oracle
+from tencirpauli_b200 import _native
+
+
+def _declared_functions() -> list:
+    header = open(os.path.join(ROOT, "include", "tcp_mvp.h")).read()
+    header = re.sub(r"/\*.*?\*/", "", header, flags=re.S)
+    return sorted(set(re.findall(r"\b(tcp_[a-z0-9_]+)\s*\(", header)))
+
+
+def test_library_loads_and_exports_every_declared_symbol() -> None:
+    lib = _native.load_library()
+    declared = _declared_functions()
+    assert declared, "no functions parsed from include/tcp_mvp.h"
+    assert set(declared) == set(_native.EXPORTED_SYMBOLS)
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert lib.tcp_abi_version() == 1
+
+
+def test_canonicalize_matches_reference_known_answers() -> None:
+    k = load_golden("canonical_known_answers")
+    for prefix in ("a", "b"):
+        codes = k[f"{prefix}_codes"]
+        n = codes.shape[1]
+        x, z, c = _native.canonicalize(n, codes, k[f"{prefix}_coefficients"])
+        ex, ez = oracle.encode_codes(n, k[f"{prefix}_expected_codes"])
+        np.testing.assert_array_equal(x, ex)
+        np.testing.assert_array_equal(z, ez)
+        np.testing.assert_array_equal(c, k[f"{prefix}_expected_coefficients"])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_canonicalize_matches_oracle_bitwise(seed: int) -> None:
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(0, 70))
+    count = int(rng.integers(0, 200))
+    # few distinct words so that duplicates (and exact cancellations) occur
+    base = rng.integers(0, 4, size=(max(1, count // 3), n)).astype(np.uint8)
+    codes = base[rng.integers(0, base.shape[0], size=count)] if count else np.zeros((0, n), np.uint8)
+    coeffs = rng.normal(size=count) + 1j * rng.normal(size=count)
+    if count > 4:
+        codes[1] = codes[0]
+        coeffs[1] = -coeffs[0]
+        coeffs[2] = 0.0
+        coeffs[3] = -0.0 + 0.0j
+    x, z, c = _native.canonicalize(n, codes, coeffs)
+    ox, oz, oc = oracle.canonicalize(n, codes, coeffs)
+    np.testing.assert_array_equal(x, ox)
+    np.testing.assert_array_equal(z, oz)
+    assert c.tobytes() == oc.tobytes()
+
+
+def test_canonicalize_error_statuses() -> None:
+    with pytest.raises(ValueError, match="invalid Pauli code 4 at index 1"):
+        _native.canonicalize(2, np.asarray([[1, 4]], np.uint8), np.asarray([1.0 + 0j]))
+    with pytest.raises(ValueError, match="coefficient at index 0 is not finite"):
+        _native.canonicalize(1, np.asarray([[1]], np.uint8), np.asarray([np.inf + 0j]))
+
+
+def test_last_error_is_thread_local_text() -> None:
+    with pytest.raises(ValueError):
+        _native.canonicalize(1, np.asarray([[9]], np.uint8), np.asarray([1.0 + 0j]))
+    assert "invalid Pauli code 9" in _native.last_error()
+
+
+def test_eager_budget_is_checked_before_any_device_use() -> None:
+    # hamiltonian.rs:84-119: G * 2^n * 16 diagonal bytes against max_bytes
+    lib = _native.load_library()
+    x = np.asarray([1], dtype=np.uint64)
+    z = np.asarray([0], dtype=np.uint64)
+    c = np.asarray([1.0, 0.0], dtype=np.float64)
+    handle = ctypes.c_void_p(None)
+    status = lib.tcp_mvp_plan_create(
+        30,
+        1,
+        1,
+        x.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+        z.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+        c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        _native.TCP_STORAGE_EAGER,
+        1 << 30,
+        ctypes.byref(handle),
+    )
+    assert status == _native.TCP_ERR_MEMORY_LIMIT
+    assert "exceeds memory limit 1073741824" in _native.last_error()
+    assert handle.value is None
+
+
+def test_plan_create_argument_errors() -> None:
+    lib = _native.load_library()
+    handle = ctypes.c_void_p(None)
+    x = np.zeros(2, np.uint64)
+    c = np.zeros(2, np.float64)
+    p64 = ctypes.POINTER(ctypes.c_uint64)
+    pf = ctypes.POINTER(ctypes.c_double)
+    # bad storage label -> InvalidSector
+    assert (
+        lib.tcp_mvp_plan_create(2, 1, 1, x.ctypes.data_as(p64), x.ctypes.data_as(p64), c.ctypes.data_as(pf), 7, 0, ctypes.byref(handle))
+        == _native.TCP_ERR_INVALID_SECTOR
+    )
+    # wrong packed word count -> InvalidWordLength (pauli_action.rs:38-50)
+    assert (
+        lib.tcp_mvp_plan_create(2, 1, 2, x.ctypes.data_as(p64), x.ctypes.data_as(p64), c.ctypes.data_as(pf), 0, 0, ctypes.byref(handle))
+        == _native.TCP_ERR_INVALID_WORD_LENGTH
+    )
+    assert "expected 1 packed words, got 2" in _native.last_error()
+    # n >= 64 -> Overflow
+    assert (
+        lib.tcp_mvp_plan_create(64, 1, 1, x.ctypes.data_as(p64), x.ctypes.data_as(p64), c.ctypes.data_as(pf), 0, 0, ctypes.byref(handle))
+        == _native.TCP_ERR_OVERFLOW
+    )
+    # non-finite coefficient
+    bad = np.asarray([np.nan, 0.0])
+    assert (
+        lib.tcp_mvp_plan_create(2, 1, 1, x.ctypes.data_as(p64), x.ctypes.data_as(p64), bad.ctypes.data_as(pf), 0, 0, ctypes.byref(handle))
+        == _native.TCP_ERR_NON_FINITE_COEFFICIENT
+    )
+    assert lib.tcp_mvp_plan_create(2, 0, 1, None, None, None, 0, 0, None) == _native.TCP_ERR_INVALID_ARGUMENT
