@@ -48,7 +48,7 @@ def _assert_fp64_close(y: np.ndarray, ref: np.ndarray) -> None:
 def test_golden_vectors(name: str, storage: str) -> None:
     g = load_golden(name)
     n = int(g["nqubits"])
-    op = PauliOperator.from_code_arrays(g["codes"].reshape(-1, n), g["coefficients"])
+    op = PauliOperator.from_code_arrays(g["codes"].reshape(len(g["coefficients"]), n), g["coefficients"])
     plan = op.native_mvp_plan(storage=storage)
     y = plan.apply(g["state"])
     np.testing.assert_allclose(y, g["expected"], rtol=1e-12, atol=1e-12)
