@@ -153,6 +153,34 @@ int tcp_mvp_apply_into_host_c64(const tcp_mvp_plan *plan, const float *state,
 int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
                               uint64_t len, uint32_t nrhs, int dtype, void *stream);
 
+/*
+ * Allocation-free host apply.  This entry point has no counterpart in the
+ * reference; it exists for callers that must not allocate device memory while
+ * they apply, such as applications whose own allocator owns the GPU's memory
+ * and forbids allocations behind its back, or services that reserve every
+ * allocation at start-up and may not touch the allocator afterwards.
+ * tcp_mvp_apply_into_host allocates a device workspace on its first call;
+ * this variant calls no cudaMalloc/cudaFree (nor any allocating routine) and
+ * instead stages the state and the result through one fixed device array that
+ * is part of the library image: TCP_NOALLOC_MAX_QUBITS = 20, i.e. two vectors
+ * of 2^20 complex128 (32 MiB + 256 bytes), which every GPU that loads the
+ * library holds until the process exits.  Plans with more qubits are rejected
+ * with TCP_ERR_MEMORY_LIMIT.  The plan itself must still be created
+ * beforehand (tcp_mvp_plan_create allocates it).
+ *  - The first call on a device looks up the array's device address
+ *    (set-up); make that first call before any stream capture.
+ *  - Every call shares the one array: calls that overlap on the GPU (from
+ *    several host threads, or several streams) race and must be serialised
+ *    by the caller.  The array keeps the last call's contents.
+ *  - Runs on `stream` (a cudaStream_t, NULL for the legacy default stream) and
+ *    returns after the result is in `result`.  Semantics otherwise equal
+ *    tcp_mvp_apply_into_host (lengths, overwrite, errors).
+ */
+#define TCP_NOALLOC_MAX_QUBITS 20
+int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const double *state,
+                                    uint64_t state_len, double *result, uint64_t result_len,
+                                    void *stream);
+
 /* Synchronise the plan's device and report (then clear) any device-side error
  * flag raised by kernels of this plan. */
 int tcp_mvp_plan_device_status(const tcp_mvp_plan *plan);

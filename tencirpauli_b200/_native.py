@@ -55,6 +55,7 @@ EXPORTED_SYMBOLS = (
     "tcp_mvp_apply_into_host",
     "tcp_mvp_apply_into_host_c64",
     "tcp_mvp_apply_into_device",
+    "tcp_mvp_apply_into_host_noalloc",
     "tcp_mvp_plan_device_status",
     "tcp_mvp_transition_count",
     "tcp_mvp_diagonal_device",
@@ -113,6 +114,7 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mvp_apply_into_host.argtypes = [vp, f64p, u64, f64p, u64, u64]
         lib.tcp_mvp_apply_into_host_c64.argtypes = [vp, f32p, u64, f32p, u64]
         lib.tcp_mvp_apply_into_device.argtypes = [vp, vp, vp, u64, u32, i32, vp]
+        lib.tcp_mvp_apply_into_host_noalloc.argtypes = [vp, f64p, u64, f64p, u64, vp]
         lib.tcp_mvp_plan_device_status.argtypes = [vp]
         lib.tcp_mvp_transition_count.argtypes = [vp, u64p]
         lib.tcp_mvp_diagonal_device.argtypes = [vp, vp, u64, vp]

@@ -713,3 +713,97 @@ extern "C" int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, u
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "diagonal kernel launch");
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free host apply (tcp_mvp_apply_into_host_noalloc).
+//
+// For callers that may not allocate device memory while applying.  The state
+// and the result are staged through one static device array that belongs to
+// the library image: a 256-byte status block (cleared at the start of every
+// call) followed by two vectors of 2^TCP_NOALLOC_MAX_QUBITS complex128.  Every
+// GPU that loads the library holds it (32 MiB + 256 B) until the process exits.
+// All calls share it, so calls that overlap on the GPU race; it keeps the last
+// call's contents.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoallocStatusBytes = 256;
+constexpr size_t kNoallocMaxDim = size_t(1) << TCP_NOALLOC_MAX_QUBITS;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocStatusBytes + 2 * kNoallocMaxDim * sizeof(double2)];
+
+std::mutex g_noalloc_mutex;
+unsigned char *g_noalloc_ptr[64] = {};
+bool g_noalloc_attr[64] = {};
+
+// Set-up, once per device, with that device current: the host-side name of a
+// __device__ array is only a stand-in, so its device address is looked up.
+int noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= 64) return fail(TCP_ERR_WRONG_DEVICE, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_ptr[device] == nullptr) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress of the static scratch");
+        g_noalloc_ptr[device] = static_cast<unsigned char *>(p);
+    }
+    if (!g_noalloc_attr[device]) {
+        int st = set_smem_attr<kLogRowsC128, double>();
+        if (st) return st;
+        g_noalloc_attr[device] = true;
+    }
+    *out = g_noalloc_ptr[device];
+    return TCP_OK;
+}
+
+}  // namespace
+
+extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const double *state, uint64_t state_len,
+                                               double *result, uint64_t result_len, void *stream) {
+    int st = check_plan(plan);
+    if (st) return st;
+    if (state_len != plan->dim) return length_error(plan->dim, state_len);
+    if (result_len != plan->dim) return length_error(plan->dim, result_len);
+    if (state == nullptr || result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    if (plan->nqubits > TCP_NOALLOC_MAX_QUBITS) {
+        return fail(TCP_ERR_MEMORY_LIMIT,
+                    "tcp_mvp_apply_into_host_noalloc handles at most " + std::to_string(TCP_NOALLOC_MAX_QUBITS) +
+                        " qubits (static scratch of 2^" + std::to_string(TCP_NOALLOC_MAX_QUBITS) +
+                        " amplitudes per vector); this plan has " + std::to_string(plan->nqubits));
+    }
+    const size_t bytes = plan->dim * sizeof(double2);
+    if (overlaps(state, result, bytes)) return fail(TCP_ERR_INVALID_ARGUMENT, "input and output must not overlap");
+    unsigned char *base = nullptr;
+    st = noalloc_scratch(plan->device, &base);
+    if (st) return st;
+    int *d_status = reinterpret_cast<int *>(base);
+    double2 *dx = reinterpret_cast<double2 *>(base + kNoallocStatusBytes);
+    double2 *dy = dx + kNoallocMaxDim;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    cudaError_t e = cudaMemsetAsync(d_status, 0, kNoallocStatusBytes, s);  // must start at zero
+    if (e != cudaSuccess) return cuda_fail(e, "clearing the static scratch status");
+    e = cudaMemcpyAsync(dx, state, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "H2D copy into the static scratch");
+    const DeviceSchedule &ds = plan->c128;
+    const uint32_t S = kTileBitsC128;
+    if (plan->nqubits >= S && ds.host.tile_bits == S) {
+        const size_t smem = 2 * (size_t(1) << S) * sizeof(double2);
+        k_tiled<kLogRowsC128, double><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(ds.dev, dx, dy,
+                                                                                                  d_status);
+    } else {
+        const int threads = 256;
+        const uint64_t blocks = (plan->dim + threads - 1) / threads;
+        k_rowwise<double><<<static_cast<unsigned>(blocks), threads, 0, s>>>(ds.dev, dx, dy, plan->dim);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "MVP kernel launch");
+    e = cudaMemcpyAsync(result, dy, bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(e, "D2H copy from the static scratch");
+    int h_status = 0;
+    e = cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(e, "reading the static scratch status");
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+    if (h_status & kErrTimeout) return fail(TCP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+    return TCP_OK;
+}
