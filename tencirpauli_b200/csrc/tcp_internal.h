@@ -31,22 +31,44 @@ struct MatrixTerm {
 // index XOR d) and an inner mask m & (2^tile_bits - 1) (a permutation inside
 // the tile).  A "step" is one distinct outer pattern with all groups that share
 // it; one tile load serves every group of a step.
+//
+// Inside a tile, thread t of a CTA with 2^log_threads threads owns rows
+// t + j * 2^log_threads (j = 0 .. 2^(tile_bits-log_threads) - 1).  For group
+// inner mask m the thread reads source rows (t ^ (m & (T-1))) + jj * T and row
+// j takes source jj = j ^ (m >> log_threads).  The sign of a term at source
+// column c = (tile ^ d) * 2^S + local is
+//   parity(zt & tile) ^ parity(zt & d) ^ parity(zlo & (t ^ m_lo)) ^ parity(zj & jj)
+// with zt = z >> S, zlo = z & (T-1), zj = (z & (2^S-1)) >> log_threads.  The
+// schedule folds parity(zt & d) into the term's weight, stores the 2^(S-logT)
+// bit pattern parity(zj & jj) per term, and leaves the two per-thread parities
+// to the kernel.
 struct Schedule {
     uint32_t tile_bits = 0;
+    uint32_t log_threads = 0;
+    // step view (tiled kernels)
     std::vector<uint64_t> step_d;     // outer pattern, as a tile-index XOR
     std::vector<uint32_t> step_gbeg;  // groups of step s: [step_gbeg[s], step_gbeg[s+1])
-    std::vector<uint32_t> g_min;      // inner mask of each group
+    std::vector<uint32_t> g_rec;      // per group: inner mask, first term, end term, 0
+    std::vector<uint64_t> t_rec;      // per term: (zlo | pattern << 32 | kind << 56), zt
+    std::vector<double> t_ws;         // weight with parity(zt & d) folded in (re, im)
+    std::vector<float> t_wfs;         // the same rounded to FP32
+    // group view (row kernel, transition count, diagonal): unfolded
+    std::vector<uint64_t> g_mask;     // full x mask per group (schedule order)
     std::vector<uint32_t> g_tbeg;     // terms of group g: [g_tbeg[g], g_tbeg[g+1])
     std::vector<uint64_t> t_z;        // z mask of each term, schedule order
     std::vector<double> t_w;          // weighted phase (re, im), schedule order
     std::vector<float> t_wf;          // the same rounded to FP32 (re, im)
 };
 
+// Term kinds (uniform per term): the weight is real, imaginary, or general.
+enum : uint32_t { kKindReal = 0, kKindImag = 1, kKindComplex = 2 };
+
 // Build the schedule for one tile width.  Groups are the distinct x masks
 // (group_matrix_terms, hamiltonian.rs:573-582); terms keep canonical order
 // inside a group so the per-group diagonal sum rounds exactly as the
 // reference's eager diagonal (hamiltonian.rs:125-133).
-Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits);
+Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits,
+                        uint32_t log_threads);
 
 // Compile packed words into matrix terms (pauli_action.rs:24-88).
 int compile_terms(uint32_t nqubits, uint64_t count, uint32_t word_count, const uint64_t *x_words,

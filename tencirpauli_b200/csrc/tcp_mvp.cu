@@ -36,7 +36,7 @@ namespace {
 constexpr int kLogThreads = 9;               // 512 threads per CTA
 constexpr int kThreads = 1 << kLogThreads;
 constexpr int kLogRowsC128 = 3;              // 8 rows per thread  -> 4096-row tile
-constexpr int kLogRowsC64 = 4;               // 16 rows per thread -> 8192-row tile
+constexpr int kLogRowsC64 = 3;               // 8 rows per thread  -> 4096-row tile
 constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
 constexpr uint32_t kTileBitsC64 = kLogThreads + kLogRowsC64;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
@@ -45,15 +45,22 @@ constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any 
 constexpr int kErrTimeout = 1;
 
 struct DevSchedule {
+    // step view (tiled kernels); see tcp::Schedule
     const uint64_t *step_d;
     const uint32_t *step_gbeg;
-    const uint32_t *g_min;
+    const uint4 *g_rec;         // inner mask, first term, end term, 0
+    const ulonglong2 *t_rec;    // (zlo | pattern << 32 | kind << 56, zt)
+    const double2 *t_ws;        // weights with the outer-pattern parity folded in
+    const float2 *t_wfs;
+    uint32_t nsteps;
+    uint32_t tile_bits;
+    // group view (row kernel, transition count, diagonal): unfolded weights
+    const uint64_t *g_mask;
     const uint32_t *g_tbeg;
     const uint64_t *t_z;
     const double2 *t_w;
     const float2 *t_wf;
-    uint32_t nsteps;
-    uint32_t tile_bits;
+    uint32_t ngroups;
 };
 
 // ------------------------------- PTX helpers -------------------------------
@@ -118,51 +125,136 @@ template <> __device__ __forceinline__ double2 weight_of<double>(const DevSchedu
 template <> __device__ __forceinline__ float2 weight_of<float>(const DevSchedule &s, uint32_t t) {
     return __ldg(&s.t_wf[t]);
 }
+template <typename R> __device__ __forceinline__ typename Cx<R>::T step_weight_of(const DevSchedule &s, uint32_t t);
+template <> __device__ __forceinline__ double2 step_weight_of<double>(const DevSchedule &s, uint32_t t) {
+    return __ldg(&s.t_ws[t]);
+}
+template <> __device__ __forceinline__ float2 step_weight_of<float>(const DevSchedule &s, uint32_t t) {
+    return __ldg(&s.t_wfs[t]);
+}
 
-// Accumulator of one output row: FP64 plain sum, FP32 Kahan-compensated sum
-// (one compensation term per component, carried across x-mask groups).
+// Flip the sign of w when bit `bit` of `pattern` is set (an integer op on the
+// sign bit; `bit` is a compile-time constant after unrolling).
+__device__ __forceinline__ double flip_if(double w, uint32_t pattern, int bit) {
+    const int hi = __double2hiint(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u);
+    return __hiloint2double(hi, __double2loint(w));
+}
+__device__ __forceinline__ float flip_if(float w, uint32_t pattern, int bit) {
+    return __int_as_float(__float_as_int(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u));
+}
+
+// Accumulator of one output row.  FP64: terms are added straight into the
+// row sum.  FP32: a group's terms are summed into a temporary, and the group's
+// total is added to the row sum with Kahan compensation (one compensation
+// term per component, carried across x-mask groups).
 template <typename R> struct Acc;
 template <> struct Acc<double> {
     double re = 0.0, im = 0.0;
-    __device__ __forceinline__ void add_product(double dre, double dim, double2 v) {
-        re = fma(dre, v.x, re);
-        re = fma(-dim, v.y, re);
-        im = fma(dre, v.y, im);
-        im = fma(dim, v.x, im);
+    __device__ __forceinline__ void begin_group() {}
+    __device__ __forceinline__ void end_group() {}
+    __device__ __forceinline__ void add_real(double w, double2 v) {
+        re = fma(w, v.x, re);
+        im = fma(w, v.y, im);
     }
+    __device__ __forceinline__ void add_imag(double w, double2 v) {
+        re = fma(-w, v.y, re);
+        im = fma(w, v.x, im);
+    }
+    __device__ __forceinline__ void add_complex(double wr, double wi, double2 v) {
+        re = fma(wr, v.x, re);
+        re = fma(-wi, v.y, re);
+        im = fma(wr, v.y, im);
+        im = fma(wi, v.x, im);
+    }
+    // group view: D = sum of signed weights, then y += D x
+    __device__ __forceinline__ void add_product(double dre, double dim, double2 v) { add_complex(dre, dim, v); }
     __device__ __forceinline__ double2 value() const { return make_double2(re, im); }
 };
 template <> struct Acc<float> {
-    float re = 0.f, im = 0.f, cre = 0.f, cim = 0.f;
+    float re = 0.f, im = 0.f, cre = 0.f, cim = 0.f;  // Kahan sums
+    float pre = 0.f, pim = 0.f;                      // current group's contribution
     __device__ __forceinline__ static void kahan(float &sum, float &comp, float term) {
-        float yv = term - comp;
-        float tv = __fadd_rn(sum, yv);
+        const float yv = __fsub_rn(term, comp);
+        const float tv = __fadd_rn(sum, yv);
         comp = __fsub_rn(__fsub_rn(tv, sum), yv);
         sum = tv;
     }
-    __device__ __forceinline__ void add_product(float dre, float dim, float2 v) {
-        float pre = __fmaf_rn(dre, v.x, -dim * v.y);
-        float pim = __fmaf_rn(dre, v.y, dim * v.x);
+    __device__ __forceinline__ void begin_group() { pre = pim = 0.f; }
+    __device__ __forceinline__ void end_group() {
         kahan(re, cre, pre);
         kahan(im, cim, pim);
+    }
+    __device__ __forceinline__ void add_real(float w, float2 v) {
+        pre = __fmaf_rn(w, v.x, pre);
+        pim = __fmaf_rn(w, v.y, pim);
+    }
+    __device__ __forceinline__ void add_imag(float w, float2 v) {
+        pre = __fmaf_rn(-w, v.y, pre);
+        pim = __fmaf_rn(w, v.x, pim);
+    }
+    __device__ __forceinline__ void add_complex(float wr, float wi, float2 v) {
+        pre = __fmaf_rn(wr, v.x, pre);
+        pre = __fmaf_rn(-wi, v.y, pre);
+        pim = __fmaf_rn(wr, v.y, pim);
+        pim = __fmaf_rn(wi, v.x, pim);
+    }
+    __device__ __forceinline__ void add_product(float dre, float dim, float2 v) {
+        begin_group();
+        add_complex(dre, dim, v);
+        end_group();
     }
     __device__ __forceinline__ float2 value() const { return make_float2(re, im); }
 };
 
 // --------------------------------- kernels ---------------------------------
-// Tile-staged grouped MVP (see file header).  Grid: one CTA per output tile.
+// Terms of one x-mask group applied to the thread's E rows.  JH (the group's
+// inner-mask bits above the thread index) is a template parameter, so row j
+// reads the loaded source value jj = j ^ JH at a compile-time register index.
+template <int JH, int LOGE, typename R>
+__device__ __forceinline__ void apply_group(const DevSchedule &s, uint32_t tb, uint32_t te, uint32_t tl, uint64_t tile,
+                                            const typename Cx<R>::T (&xv)[1 << LOGE], Acc<R> (&acc)[1 << LOGE]) {
+    using C = typename Cx<R>::T;
+    constexpr int E = 1 << LOGE;
+    constexpr uint32_t kPatMask = (1u << E) - 1u;
+#pragma unroll
+    for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].begin_group();
+    for (uint32_t t = tb; t < te; ++t) {
+        const ulonglong2 rec = __ldg(&s.t_rec[t]);
+        const C w = step_weight_of<R>(s, t);
+        const uint32_t zlo = static_cast<uint32_t>(rec.x);
+        const uint32_t hi = static_cast<uint32_t>(rec.x >> 32);
+        const uint32_t base = (__popc(zlo & tl) + __popcll(rec.y & tile)) & 1u;
+        const uint32_t pat = (hi ^ (0u - base)) & kPatMask;  // sign bit of every source jj
+        const uint32_t kind = hi >> 24;
+        if (kind == tcp::kKindReal) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(flip_if(w.x, pat, jj), xv[jj]);
+        } else if (kind == tcp::kKindImag) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(flip_if(w.y, pat, jj), xv[jj]);
+        } else {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_complex(flip_if(w.x, pat, jj), flip_if(w.y, pat, jj), xv[jj]);
+        }
+    }
+#pragma unroll
+    for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].end_group();
+}
+
+// Tile-staged grouped MVP (see file header).  Grid: one CTA per output tile;
+// thread t owns rows t + j * kThreads of the tile.
 template <int LOGE, typename R>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tiled(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
             int *__restrict__ err) {
     using C = typename Cx<R>::T;
+    static_assert(LOGE == 3, "the group dispatch below covers 8 rows per thread");
     constexpr int E = 1 << LOGE;
     constexpr int S = kLogThreads + LOGE;
     constexpr uint32_t TILE = 1u << S;
     constexpr uint32_t BYTES = TILE * sizeof(C);
-    constexpr int CH = 4;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    C *buf[2] = {reinterpret_cast<C *>(smem_raw), reinterpret_cast<C *>(smem_raw) + TILE};
+    C *buf0 = reinterpret_cast<C *>(smem_raw);
     __shared__ __align__(8) uint64_t bars[2];
 
     const uint32_t tid = threadIdx.x;
@@ -177,13 +269,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     if (tid == 0 && nsteps > 0) {
         mbar_arrive_expect_tx(&bars[0], BYTES);
-        bulk_copy_g2s(buf[0], x + ((tile ^ s.step_d[0]) << S), BYTES, &bars[0]);
+        bulk_copy_g2s(buf0, x + ((tile ^ s.step_d[0]) << S), BYTES, &bars[0]);
     }
 
     Acc<R> acc[E];
     for (uint32_t st = 0; st < nsteps; ++st) {
         const uint32_t b = st & 1u;
-        bool ok = mbar_wait_bounded(&bars[b], (st >> 1) & 1u);
+        const bool ok = mbar_wait_bounded(&bars[b], (st >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(err, kErrTimeout);
             return;
@@ -192,42 +284,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (tid == 0 && st + 1 < nsteps) {
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&bars[b ^ 1u], BYTES);
-            bulk_copy_g2s(buf[b ^ 1u], x + ((tile ^ s.step_d[st + 1]) << S), BYTES, &bars[b ^ 1u]);
+            bulk_copy_g2s(buf0 + (b ^ 1u) * TILE, x + ((tile ^ s.step_d[st + 1]) << S), BYTES, &bars[b ^ 1u]);
         }
-        const C *xs = buf[b];
-        const uint64_t src_base = (tile ^ s.step_d[st]) << S;
+        const C *xs = buf0 + b * TILE;
         const uint32_t gb = s.step_gbeg[st], ge = s.step_gbeg[st + 1];
         for (uint32_t g = gb; g < ge; ++g) {
-            const uint32_t m = __ldg(&s.g_min[g]);
-            const uint32_t tl = tid ^ (m & (kThreads - 1));
-            const uint32_t jh = m >> kLogThreads;
-            const uint32_t tb = __ldg(&s.g_tbeg[g]), te = __ldg(&s.g_tbeg[g + 1]);
-            // Rows are processed CH at a time to bound register use.
+            const uint4 gr = __ldg(&s.g_rec[g]);
+            const uint32_t tl = tid ^ (gr.x & (kThreads - 1));
+            const uint32_t jh = gr.x >> kLogThreads;
+            C xv[E];
+            const C *src = xs + tl;
 #pragma unroll
-            for (int j0 = 0; j0 < E; j0 += CH) {
-                uint32_t col[CH];
-                C xv[CH];
-                R dre[CH], dim[CH];
-#pragma unroll
-                for (int jj = 0; jj < CH; ++jj) {
-                    col[jj] = tl | ((static_cast<uint32_t>(j0 + jj) ^ jh) << kLogThreads);
-                    xv[jj] = xs[col[jj]];
-                    dre[jj] = dim[jj] = R(0);
-                }
-                for (uint32_t t = tb; t < te; ++t) {
-                    const uint64_t z = __ldg(&s.t_z[t]);
-                    const C w = weight_of<R>(s, t);
-                    const uint32_t ph = static_cast<uint32_t>(__popcll(z & src_base));
-                    const uint32_t zl = static_cast<uint32_t>(z) & (TILE - 1);
-#pragma unroll
-                    for (int jj = 0; jj < CH; ++jj) {
-                        const bool neg = (__popc(zl & col[jj]) + ph) & 1u;
-                        dre[jj] = dre[jj] + (neg ? -w.x : w.x);
-                        dim[jj] = dim[jj] + (neg ? -w.y : w.y);
-                    }
-                }
-#pragma unroll
-                for (int jj = 0; jj < CH; ++jj) acc[j0 + jj].add_product(dre[jj], dim[jj], xv[jj]);
+            for (int jj = 0; jj < E; ++jj) xv[jj] = src[jj << kLogThreads];
+            switch (jh) {
+            case 0: apply_group<0, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 1: apply_group<1, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 2: apply_group<2, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 3: apply_group<3, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 4: apply_group<4, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 5: apply_group<5, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 6: apply_group<6, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            default: apply_group<7, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
             }
         }
     }
@@ -241,24 +318,20 @@ template <typename R>
 __global__ void k_rowwise(DevSchedule s, const typename Cx<R>::T *__restrict__ x,
                           typename Cx<R>::T *__restrict__ y, uint64_t dim) {
     using C = typename Cx<R>::T;
-    const uint32_t S = s.tile_bits;
     for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; r < dim;
          r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         Acc<R> acc;
-        for (uint32_t st = 0; st < s.nsteps; ++st) {
-            const uint64_t outer = s.step_d[st] << S;
-            for (uint32_t g = s.step_gbeg[st]; g < s.step_gbeg[st + 1]; ++g) {
-                const uint64_t c = r ^ (outer | s.g_min[g]);
-                const C v = x[c];
-                R dre = R(0), dimv = R(0);
-                for (uint32_t t = s.g_tbeg[g]; t < s.g_tbeg[g + 1]; ++t) {
-                    const C w = weight_of<R>(s, t);
-                    const bool neg = __popcll(s.t_z[t] & c) & 1;
-                    dre = dre + (neg ? -w.x : w.x);
-                    dimv = dimv + (neg ? -w.y : w.y);
-                }
-                acc.add_product(dre, dimv, v);
+        for (uint32_t g = 0; g < s.ngroups; ++g) {
+            const uint64_t c = r ^ s.g_mask[g];
+            const C v = x[c];
+            R dre = R(0), dimv = R(0);
+            for (uint32_t t = s.g_tbeg[g]; t < s.g_tbeg[g + 1]; ++t) {
+                const C w = weight_of<R>(s, t);
+                const bool neg = __popcll(s.t_z[t] & c) & 1;
+                dre = dre + (neg ? -w.x : w.x);
+                dimv = dimv + (neg ? -w.y : w.y);
             }
+            acc.add_product(dre, dimv, v);
         }
         y[r] = acc.value();
     }
@@ -367,13 +440,18 @@ int upload(tcp_mvp_plan *p) {
         tcp::Schedule &h = ds->host;
         add(h.step_d.data(), h.step_d.size() * 8, reinterpret_cast<const void **>(&ds->dev.step_d));
         add(h.step_gbeg.data(), h.step_gbeg.size() * 4, reinterpret_cast<const void **>(&ds->dev.step_gbeg));
-        add(h.g_min.data(), h.g_min.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_min));
+        add(h.g_rec.data(), h.g_rec.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_rec));
+        add(h.t_rec.data(), h.t_rec.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_rec));
+        add(h.t_ws.data(), h.t_ws.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_ws));
+        add(h.t_wfs.data(), h.t_wfs.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wfs));
+        add(h.g_mask.data(), h.g_mask.size() * 8, reinterpret_cast<const void **>(&ds->dev.g_mask));
         add(h.g_tbeg.data(), h.g_tbeg.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_tbeg));
         add(h.t_z.data(), h.t_z.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_z));
         add(h.t_w.data(), h.t_w.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_w));
         add(h.t_wf.data(), h.t_wf.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wf));
         ds->dev.nsteps = static_cast<uint32_t>(h.step_d.size());
         ds->dev.tile_bits = h.tile_bits;
+        ds->dev.ngroups = static_cast<uint32_t>(h.g_mask.size());
     }
     size_t total = 256;  // error word first
     for (auto &pc : pieces) total = align_up(total, 256) + std::max<size_t>(pc.bytes, 16);
@@ -582,8 +660,8 @@ extern "C" int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (g_num_sms == 0) cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, p->device);
-    p->c128.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128);
-    p->c64.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC64);
+    p->c128.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
+    p->c64.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC64, kLogThreads);
     st = upload(p.get());
     if (st) return st;
     if (storage == TCP_STORAGE_EAGER) {
@@ -683,7 +761,7 @@ extern "C" int tcp_mvp_transition_count(const tcp_mvp_plan *plan, uint64_t *out_
         return fail(TCP_ERR_ALLOCATION, "device allocation of the transition counter failed");
     }
     cudaMemset(d_count, 0, sizeof(unsigned long long));
-    const uint32_t ngroups = static_cast<uint32_t>(plan->c128.host.g_min.size());
+    const uint32_t ngroups = static_cast<uint32_t>(plan->c128.host.g_mask.size());
     const uint64_t total = static_cast<uint64_t>(ngroups) * plan->dim;
     if (total > 0) {
         const int threads = 256;
@@ -705,7 +783,12 @@ extern "C" int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, u
     if (d_diag == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     const tcp::Schedule &h = plan->c128.host;
     uint32_t gzero = 0xffffffffu;
-    if (!h.step_d.empty() && h.step_d[0] == 0 && !h.g_min.empty() && h.g_min[0] == 0) gzero = 0;
+    for (size_t g = 0; g < h.g_mask.size(); ++g) {
+        if (h.g_mask[g] == 0) {
+            gzero = static_cast<uint32_t>(g);
+            break;
+        }
+    }
     const int threads = 256;
     uint64_t blocks = std::min<uint64_t>((plan->dim + threads - 1) / threads, 1u << 20);
     k_diagonal<<<static_cast<unsigned>(blocks), threads, 0, static_cast<cudaStream_t>(stream)>>>(

@@ -96,11 +96,16 @@ uint64_t distinct_x_masks(const std::vector<MatrixTerm> &terms) {
     return static_cast<uint64_t>(std::unique(m.begin(), m.end()) - m.begin());
 }
 
-Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits) {
+Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits,
+                        uint32_t log_threads) {
     Schedule s;
     s.tile_bits = std::min(tile_bits, nqubits);
+    s.log_threads = std::min(log_threads, s.tile_bits);
     const uint32_t S = s.tile_bits;
+    const uint32_t L = s.log_threads;
     const uint64_t inner = (S >= 64) ? ~0ull : ((1ull << S) - 1);
+    const uint32_t jbits = S - L;
+    const uint32_t jcount = 1u << jbits;
     // (outer, inner, canonical index): a stable order that keeps canonical
     // term order inside every x-mask group.
     std::vector<uint64_t> order(terms.size());
@@ -115,24 +120,51 @@ Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, 
     for (size_t i = 0; i < order.size(); ++i) {
         const MatrixTerm &t = terms[order[i]];
         uint64_t d = t.x_mask >> S;
-        uint32_t m = static_cast<uint32_t>(t.x_mask & inner);
         bool new_step = s.step_d.empty() || s.step_d.back() != d;
-        bool new_group = new_step || s.g_min.back() != m;
-        if (new_group && !s.g_min.empty()) s.g_tbeg.push_back(static_cast<uint32_t>(s.t_z.size()));
-        if (new_step) {
-            if (!s.step_d.empty()) s.step_gbeg.push_back(static_cast<uint32_t>(s.g_min.size()));
-            s.step_d.push_back(d);
+        bool new_group = new_step || s.g_mask.back() != t.x_mask;
+        uint32_t tindex = static_cast<uint32_t>(s.t_z.size());
+        if (new_group) {
+            if (!s.g_mask.empty()) {
+                s.g_tbeg.push_back(tindex);
+                s.g_rec[s.g_rec.size() - 2] = tindex;  // end term of the previous group
+            }
+            if (new_step) {
+                if (!s.step_d.empty()) s.step_gbeg.push_back(static_cast<uint32_t>(s.g_mask.size()));
+                s.step_d.push_back(d);
+            }
+            s.g_mask.push_back(t.x_mask);
+            s.g_rec.push_back(static_cast<uint32_t>(t.x_mask & inner));
+            s.g_rec.push_back(tindex);
+            s.g_rec.push_back(tindex);  // end, patched when the group closes
+            s.g_rec.push_back(0);
         }
-        if (new_group) s.g_min.push_back(m);
+        // per-term record
+        const uint64_t zt = (S >= 64) ? 0 : (t.z_mask >> S);
+        const uint32_t zlo = static_cast<uint32_t>(t.z_mask & ((1ull << L) - 1));
+        const uint32_t zj = static_cast<uint32_t>((t.z_mask & inner) >> L);
+        uint32_t pattern = 0;
+        for (uint32_t jj = 0; jj < jcount; ++jj) pattern |= (static_cast<uint32_t>(__builtin_popcount(zj & jj)) & 1u) << jj;
+        uint32_t kind = (t.w_im == 0.0) ? kKindReal : ((t.w_re == 0.0) ? kKindImag : kKindComplex);
+        s.t_rec.push_back(static_cast<uint64_t>(zlo) | (static_cast<uint64_t>(pattern) << 32) |
+                          (static_cast<uint64_t>(kind) << 56));
+        s.t_rec.push_back(zt);
+        const bool flip = (__builtin_popcountll(zt & d) & 1) != 0;
+        const double wr = flip ? -t.w_re : t.w_re, wi = flip ? -t.w_im : t.w_im;
+        s.t_ws.push_back(wr);
+        s.t_ws.push_back(wi);
+        s.t_wfs.push_back(static_cast<float>(wr));
+        s.t_wfs.push_back(static_cast<float>(wi));
         s.t_z.push_back(t.z_mask);
         s.t_w.push_back(t.w_re);
         s.t_w.push_back(t.w_im);
         s.t_wf.push_back(static_cast<float>(t.w_re));
         s.t_wf.push_back(static_cast<float>(t.w_im));
     }
-    if (!s.g_min.empty()) {
-        s.g_tbeg.push_back(static_cast<uint32_t>(s.t_z.size()));
-        s.step_gbeg.push_back(static_cast<uint32_t>(s.g_min.size()));
+    if (!s.g_mask.empty()) {
+        uint32_t tend = static_cast<uint32_t>(s.t_z.size());
+        s.g_tbeg.push_back(tend);
+        s.g_rec[s.g_rec.size() - 2] = tend;
+        s.step_gbeg.push_back(static_cast<uint32_t>(s.g_mask.size()));
     } else {
         s.g_tbeg.assign(1, 0);
         s.step_gbeg.assign(1, 0);
