@@ -363,7 +363,7 @@ def main() -> None:
         kern_ms = statistics.mean(kernel_ms)
         b_alg = dim * 2 * elem
         achieved = b_alg / (kern_ms / 1000.0) / 1e9
-        kernel_name = "k_tiled<3,double>" if args.dtype == "c128" else "k_tiled<4,float>"
+        kernel_name = "k_tiled<3,double>" if args.dtype == "c128" else "k_tiled<3,float>"
         traffic = _profile_traffic(kernel_name)
         line = {
             "metric": METRIC,
@@ -402,8 +402,9 @@ def main() -> None:
             "clocks": clocks,
             "plan": {
                 "groups": plan.group_count,
-                "tile_bits": int(native.info.tile_bits_c128 if args.dtype == "c128" else native.info.tile_bits_c64),
-                "steps": int(native.info.steps_c128 if args.dtype == "c128" else native.info.steps_c64),
+                "tile_bits": int(native.info.tile_bits),
+                "steps": int(native.info.steps),
+                "outer_patterns": int(native.info.outer_patterns),
             },
         }
         if world == 1 and not args.no_cpu_baseline:

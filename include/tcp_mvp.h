@@ -76,10 +76,10 @@ typedef struct tcp_mvp_plan_info_t {
     int32_t device;            /* CUDA ordinal the plan lives on */
     int64_t transition_count;  /* eager nonzero count, -1 for lazy plans (None) */
     uint64_t device_bytes;     /* device memory retained by the plan */
-    uint32_t tile_bits_c128;   /* tile width (log2 rows) of the c128 schedule */
-    uint32_t tile_bits_c64;    /* tile width (log2 rows) of the c64 schedule */
-    uint64_t steps_c128;       /* outer tile patterns in the c128 schedule */
-    uint64_t steps_c64;
+    uint32_t tile_bits;        /* log2 rows of one tile of the tiled kernel */
+    uint32_t log_threads;      /* log2 threads per tile (rows per thread = 2^(tile_bits - log_threads)) */
+    uint64_t steps;            /* tile loads per output tile (outer patterns, split at 16 KiB of term data) */
+    uint64_t outer_patterns;   /* distinct outer patterns d = x_mask >> tile_bits */
 } tcp_mvp_plan_info_t;
 
 /* Library version (TCP_ABI_VERSION) */

@@ -73,10 +73,10 @@ class TcpPlanInfo(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("transition_count", ctypes.c_int64),
         ("device_bytes", ctypes.c_uint64),
-        ("tile_bits_c128", ctypes.c_uint32),
-        ("tile_bits_c64", ctypes.c_uint32),
-        ("steps_c128", ctypes.c_uint64),
-        ("steps_c64", ctypes.c_uint64),
+        ("tile_bits", ctypes.c_uint32),
+        ("log_threads", ctypes.c_uint32),
+        ("steps", ctypes.c_uint64),
+        ("outer_patterns", ctypes.c_uint64),
     ]
 
 

@@ -45,13 +45,19 @@ struct MatrixTerm {
 struct Schedule {
     uint32_t tile_bits = 0;
     uint32_t log_threads = 0;
-    // step view (tiled kernels)
-    std::vector<uint64_t> step_d;     // outer pattern, as a tile-index XOR
-    std::vector<uint32_t> step_gbeg;  // groups of step s: [step_gbeg[s], step_gbeg[s+1])
-    std::vector<uint32_t> g_rec;      // per group: inner mask, first term, end term, 0
-    std::vector<uint64_t> t_rec;      // per term: (zlo | pattern << 32 | kind << 56), zt
-    std::vector<double> t_ws;         // weight with parity(zt & d) folded in (re, im)
-    std::vector<float> t_wfs;         // the same rounded to FP32
+    uint64_t distinct_outer = 0;      // distinct outer patterns d
+    // step view (tiled kernels).  A step is one outer pattern d and a block of
+    // its groups and terms no larger than kBlockBytesMax; a pattern with more
+    // data is split over several steps (the tile is loaded once per step).
+    // step_info: 4 words per step: d (lo, hi), block offset / 16,
+    // group count | (block bytes / 16) << 16.
+    std::vector<uint32_t> step_info;
+    // Step blocks, 16-byte aligned: group records (16 B: inner mask, first
+    // term, end term, 0) then term records (32 B: zlo | pattern << 32 |
+    // kind << 56, zt, weight).  The weight has parity(zt & d) folded in and is
+    // two doubles (complex128 blocks) or two floats + 8 pad bytes (complex64).
+    std::vector<uint8_t> blocks_c128;
+    std::vector<uint8_t> blocks_c64;
     // group view (row kernel, transition count, diagonal): unfolded
     std::vector<uint64_t> g_mask;     // full x mask per group (schedule order)
     std::vector<uint32_t> g_tbeg;     // terms of group g: [g_tbeg[g], g_tbeg[g+1])
@@ -59,6 +65,10 @@ struct Schedule {
     std::vector<double> t_w;          // weighted phase (re, im), schedule order
     std::vector<float> t_wf;          // the same rounded to FP32 (re, im)
 };
+
+constexpr uint32_t kBlockBytesMax = 16384;
+constexpr uint32_t kGroupRecBytes = 16;
+constexpr uint32_t kTermRecBytes = 32;
 
 // Term kinds (uniform per term): the weight is real, imaginary, or general.
 enum : uint32_t { kKindReal = 0, kKindImag = 1, kKindComplex = 2 };

@@ -38,7 +38,6 @@ constexpr int kThreads = 1 << kLogThreads;
 constexpr int kLogRowsC128 = 3;              // 8 rows per thread  -> 4096-row tile
 constexpr int kLogRowsC64 = 3;               // 8 rows per thread  -> 4096-row tile
 constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
-constexpr uint32_t kTileBitsC64 = kLogThreads + kLogRowsC64;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
 
 // Error bits written by kernels into the plan's device status word.
@@ -46,12 +45,9 @@ constexpr int kErrTimeout = 1;
 
 struct DevSchedule {
     // step view (tiled kernels); see tcp::Schedule
-    const uint64_t *step_d;
-    const uint32_t *step_gbeg;
-    const uint4 *g_rec;         // inner mask, first term, end term, 0
-    const ulonglong2 *t_rec;    // (zlo | pattern << 32 | kind << 56, zt)
-    const double2 *t_ws;        // weights with the outer-pattern parity folded in
-    const float2 *t_wfs;
+    const uint4 *step_info;          // d lo, d hi, block offset / 16, ngroups | (bytes / 16) << 16
+    const unsigned char *blocks128;  // step blocks with FP64 weights
+    const unsigned char *blocks64;   // step blocks with FP32 weights
     uint32_t nsteps;
     uint32_t tile_bits;
     // group view (row kernel, transition count, diagonal): unfolded weights
@@ -125,12 +121,13 @@ template <> __device__ __forceinline__ double2 weight_of<double>(const DevSchedu
 template <> __device__ __forceinline__ float2 weight_of<float>(const DevSchedule &s, uint32_t t) {
     return __ldg(&s.t_wf[t]);
 }
-template <typename R> __device__ __forceinline__ typename Cx<R>::T step_weight_of(const DevSchedule &s, uint32_t t);
-template <> __device__ __forceinline__ double2 step_weight_of<double>(const DevSchedule &s, uint32_t t) {
-    return __ldg(&s.t_ws[t]);
+// Weight of a term record in a shared-memory step block (offset 16 bytes).
+template <typename R> __device__ __forceinline__ typename Cx<R>::T record_weight(const unsigned char *rec);
+template <> __device__ __forceinline__ double2 record_weight<double>(const unsigned char *rec) {
+    return *reinterpret_cast<const double2 *>(rec + 16);
 }
-template <> __device__ __forceinline__ float2 step_weight_of<float>(const DevSchedule &s, uint32_t t) {
-    return __ldg(&s.t_wfs[t]);
+template <> __device__ __forceinline__ float2 record_weight<float>(const unsigned char *rec) {
+    return *reinterpret_cast<const float2 *>(rec + 16);
 }
 
 // Flip the sign of w when bit `bit` of `pattern` is set (an integer op on the
@@ -141,6 +138,13 @@ __device__ __forceinline__ double flip_if(double w, uint32_t pattern, int bit) {
 }
 __device__ __forceinline__ float flip_if(float w, uint32_t pattern, int bit) {
     return __int_as_float(__float_as_int(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u));
+}
+// Flip the sign of w when `odd` (0 or 1) is set.
+__device__ __forceinline__ double flip_by(double w, uint32_t odd) {
+    return __hiloint2double(__double2hiint(w) ^ static_cast<int>(odd << 31), __double2loint(w));
+}
+__device__ __forceinline__ float flip_by(float w, uint32_t odd) {
+    return __int_as_float(__float_as_int(w) ^ static_cast<int>(odd << 31));
 }
 
 // Accumulator of one output row.  FP64: terms are added straight into the
@@ -210,39 +214,82 @@ template <> struct Acc<float> {
 // Terms of one x-mask group applied to the thread's E rows.  JH (the group's
 // inner-mask bits above the thread index) is a template parameter, so row j
 // reads the loaded source value jj = j ^ JH at a compile-time register index.
+// Term records come from the step block in shared memory.  A term whose z mask
+// has no bit among the thread's row bits (pattern 0) has one sign for all E
+// rows; otherwise the sign of source jj is bit jj of the pattern.
 template <int JH, int LOGE, typename R>
-__device__ __forceinline__ void apply_group(const DevSchedule &s, uint32_t tb, uint32_t te, uint32_t tl, uint64_t tile,
-                                            const typename Cx<R>::T (&xv)[1 << LOGE], Acc<R> (&acc)[1 << LOGE]) {
+__device__ __forceinline__ void apply_group(const unsigned char *__restrict__ trm, uint32_t tb, uint32_t te,
+                                            uint32_t tl, uint64_t tile, const typename Cx<R>::T (&xv)[1 << LOGE],
+                                            Acc<R> (&acc)[1 << LOGE]) {
     using C = typename Cx<R>::T;
     constexpr int E = 1 << LOGE;
     constexpr uint32_t kPatMask = (1u << E) - 1u;
 #pragma unroll
     for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].begin_group();
     for (uint32_t t = tb; t < te; ++t) {
-        const ulonglong2 rec = __ldg(&s.t_rec[t]);
-        const C w = step_weight_of<R>(s, t);
+        const unsigned char *rp = trm + t * tcp::kTermRecBytes;
+        const ulonglong2 rec = *reinterpret_cast<const ulonglong2 *>(rp);
+        const C w = record_weight<R>(rp);
         const uint32_t zlo = static_cast<uint32_t>(rec.x);
         const uint32_t hi = static_cast<uint32_t>(rec.x >> 32);
         const uint32_t base = (__popc(zlo & tl) + __popcll(rec.y & tile)) & 1u;
-        const uint32_t pat = (hi ^ (0u - base)) & kPatMask;  // sign bit of every source jj
+        const uint32_t pattern = hi & kPatMask;
         const uint32_t kind = hi >> 24;
-        if (kind == tcp::kKindReal) {
+        if (pattern == 0u) {
+            const R wr = flip_by(w.x, base), wi = flip_by(w.y, base);
+            if (kind == tcp::kKindReal) {
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(flip_if(w.x, pat, jj), xv[jj]);
-        } else if (kind == tcp::kKindImag) {
+                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(wr, xv[jj]);
+            } else if (kind == tcp::kKindImag) {
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(flip_if(w.y, pat, jj), xv[jj]);
+                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(wi, xv[jj]);
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_complex(wr, wi, xv[jj]);
+            }
         } else {
+            const uint32_t pat = (pattern ^ (0u - base)) & kPatMask;  // sign bit of every source jj
+            if (kind == tcp::kKindReal) {
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_complex(flip_if(w.x, pat, jj), flip_if(w.y, pat, jj), xv[jj]);
+                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(flip_if(w.x, pat, jj), xv[jj]);
+            } else if (kind == tcp::kKindImag) {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(flip_if(w.y, pat, jj), xv[jj]);
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < E; ++jj)
+                    acc[jj ^ JH].add_complex(flip_if(w.x, pat, jj), flip_if(w.y, pat, jj), xv[jj]);
+            }
         }
     }
 #pragma unroll
     for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].end_group();
 }
 
+template <typename R> __device__ __forceinline__ const unsigned char *step_blocks(const DevSchedule &s);
+template <> __device__ __forceinline__ const unsigned char *step_blocks<double>(const DevSchedule &s) {
+    return s.blocks128;
+}
+template <> __device__ __forceinline__ const unsigned char *step_blocks<float>(const DevSchedule &s) {
+    return s.blocks64;
+}
+
+// Issue the bulk copies of one step (source tile + step block) on one mbarrier.
+template <typename C, uint32_t S>
+__device__ __forceinline__ void issue_step(const uint4 info, uint64_t tile, const C *__restrict__ x,
+                                           const unsigned char *__restrict__ blocks, C *tile_dst,
+                                           unsigned char *blk_dst, uint64_t *bar) {
+    constexpr uint32_t BYTES = (1u << S) * sizeof(C);
+    const uint64_t d = static_cast<uint64_t>(info.x) | (static_cast<uint64_t>(info.y) << 32);
+    const uint32_t blk_bytes = (info.w >> 16) * 16u;
+    mbar_arrive_expect_tx(bar, BYTES + blk_bytes);
+    bulk_copy_g2s(tile_dst, x + ((tile ^ d) << S), BYTES, bar);
+    bulk_copy_g2s(blk_dst, blocks + static_cast<size_t>(info.z) * 16u, blk_bytes, bar);
+}
+
 // Tile-staged grouped MVP (see file header).  Grid: one CTA per output tile;
-// thread t owns rows t + j * kThreads of the tile.
+// thread t owns rows t + j * kThreads of the tile.  Shared memory: two source
+// tiles and two step blocks (double buffering), refilled by the TMA engine.
 template <int LOGE, typename R>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tiled(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
@@ -252,14 +299,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     constexpr int E = 1 << LOGE;
     constexpr int S = kLogThreads + LOGE;
     constexpr uint32_t TILE = 1u << S;
-    constexpr uint32_t BYTES = TILE * sizeof(C);
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    C *buf0 = reinterpret_cast<C *>(smem_raw);
+    C *tiles = reinterpret_cast<C *>(smem_raw);
+    unsigned char *blks = smem_raw + 2 * TILE * sizeof(C);
     __shared__ __align__(8) uint64_t bars[2];
 
     const uint32_t tid = threadIdx.x;
     const uint64_t tile = blockIdx.x;
     const uint32_t nsteps = s.nsteps;
+    const unsigned char *blocks = step_blocks<R>(s);
 
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -267,29 +315,30 @@ __global__ void __launch_bounds__(kThreads, 1)
         fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0 && nsteps > 0) {
-        mbar_arrive_expect_tx(&bars[0], BYTES);
-        bulk_copy_g2s(buf0, x + ((tile ^ s.step_d[0]) << S), BYTES, &bars[0]);
-    }
+    if (tid == 0 && nsteps > 0) issue_step<C, S>(__ldg(&s.step_info[0]), tile, x, blocks, tiles, blks, &bars[0]);
 
     Acc<R> acc[E];
     for (uint32_t st = 0; st < nsteps; ++st) {
         const uint32_t b = st & 1u;
+        const uint4 info = __ldg(&s.step_info[st]);
         const bool ok = mbar_wait_bounded(&bars[b], (st >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(err, kErrTimeout);
             return;
         }
-        // Every thread has finished step st-1, so the other buffer is free.
+        // Every thread has finished step st-1, so the other buffers are free.
         if (tid == 0 && st + 1 < nsteps) {
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&bars[b ^ 1u], BYTES);
-            bulk_copy_g2s(buf0 + (b ^ 1u) * TILE, x + ((tile ^ s.step_d[st + 1]) << S), BYTES, &bars[b ^ 1u]);
+            issue_step<C, S>(__ldg(&s.step_info[st + 1]), tile, x, blocks, tiles + (b ^ 1u) * TILE,
+                             blks + (b ^ 1u) * tcp::kBlockBytesMax, &bars[b ^ 1u]);
         }
-        const C *xs = buf0 + b * TILE;
-        const uint32_t gb = s.step_gbeg[st], ge = s.step_gbeg[st + 1];
-        for (uint32_t g = gb; g < ge; ++g) {
-            const uint4 gr = __ldg(&s.g_rec[g]);
+        const C *xs = tiles + b * TILE;
+        const unsigned char *blk = blks + b * tcp::kBlockBytesMax;
+        const uint32_t ng = info.w & 0xffffu;
+        const uint4 *grp = reinterpret_cast<const uint4 *>(blk);
+        const unsigned char *trm = blk + ng * tcp::kGroupRecBytes;
+        for (uint32_t g = 0; g < ng; ++g) {
+            const uint4 gr = grp[g];
             const uint32_t tl = tid ^ (gr.x & (kThreads - 1));
             const uint32_t jh = gr.x >> kLogThreads;
             C xv[E];
@@ -297,14 +346,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
             for (int jj = 0; jj < E; ++jj) xv[jj] = src[jj << kLogThreads];
             switch (jh) {
-            case 0: apply_group<0, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 1: apply_group<1, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 2: apply_group<2, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 3: apply_group<3, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 4: apply_group<4, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 5: apply_group<5, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 6: apply_group<6, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
-            default: apply_group<7, LOGE, R>(s, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 0: apply_group<0, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 1: apply_group<1, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 2: apply_group<2, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 3: apply_group<3, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 4: apply_group<4, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 5: apply_group<5, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            case 6: apply_group<6, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+            default: apply_group<7, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
             }
         }
     }
@@ -413,8 +462,7 @@ struct tcp_mvp_plan {
     int64_t transitions = -1;
     std::vector<tcp::MatrixTerm> terms;
     uint64_t group_count = 0;
-    DeviceSchedule c128;
-    DeviceSchedule c64;
+    DeviceSchedule sched;  // one schedule (4096-row tiles) serves both precisions
     void *dev_block = nullptr;
     size_t dev_bytes = 0;
     int *d_err = nullptr;
@@ -436,20 +484,18 @@ int upload(tcp_mvp_plan *p) {
     };
     std::vector<Piece> pieces;
     auto add = [&](const void *src, size_t bytes, const void **dst) { pieces.push_back({src, bytes, dst}); };
-    for (DeviceSchedule *ds : {&p->c128, &p->c64}) {
+    {
+        DeviceSchedule *ds = &p->sched;
         tcp::Schedule &h = ds->host;
-        add(h.step_d.data(), h.step_d.size() * 8, reinterpret_cast<const void **>(&ds->dev.step_d));
-        add(h.step_gbeg.data(), h.step_gbeg.size() * 4, reinterpret_cast<const void **>(&ds->dev.step_gbeg));
-        add(h.g_rec.data(), h.g_rec.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_rec));
-        add(h.t_rec.data(), h.t_rec.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_rec));
-        add(h.t_ws.data(), h.t_ws.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_ws));
-        add(h.t_wfs.data(), h.t_wfs.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wfs));
+        add(h.step_info.data(), h.step_info.size() * 4, reinterpret_cast<const void **>(&ds->dev.step_info));
+        add(h.blocks_c128.data(), h.blocks_c128.size(), reinterpret_cast<const void **>(&ds->dev.blocks128));
+        add(h.blocks_c64.data(), h.blocks_c64.size(), reinterpret_cast<const void **>(&ds->dev.blocks64));
         add(h.g_mask.data(), h.g_mask.size() * 8, reinterpret_cast<const void **>(&ds->dev.g_mask));
         add(h.g_tbeg.data(), h.g_tbeg.size() * 4, reinterpret_cast<const void **>(&ds->dev.g_tbeg));
         add(h.t_z.data(), h.t_z.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_z));
         add(h.t_w.data(), h.t_w.size() * 8, reinterpret_cast<const void **>(&ds->dev.t_w));
         add(h.t_wf.data(), h.t_wf.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wf));
-        ds->dev.nsteps = static_cast<uint32_t>(h.step_d.size());
+        ds->dev.nsteps = static_cast<uint32_t>(h.step_info.size() / 4);
         ds->dev.tile_bits = h.tile_bits;
         ds->dev.ngroups = static_cast<uint32_t>(h.g_mask.size());
     }
@@ -502,8 +548,12 @@ bool overlaps(const void *a, const void *b, size_t bytes) {
     return pa < pb + bytes && pb < pa + bytes;
 }
 
+template <int LOGE, typename R> constexpr size_t tiled_smem_bytes() {
+    return 2 * (size_t(1) << (kLogThreads + LOGE)) * sizeof(typename Cx<R>::T) + 2 * size_t(tcp::kBlockBytesMax);
+}
+
 template <int LOGE, typename R> int set_smem_attr() {
-    constexpr size_t bytes = 2 * (size_t(1) << (kLogThreads + LOGE)) * sizeof(typename Cx<R>::T);
+    constexpr size_t bytes = tiled_smem_bytes<LOGE, R>();
     cudaError_t e = cudaFuncSetAttribute(k_tiled<LOGE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "cudaFuncSetAttribute");
@@ -515,7 +565,7 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
     using C = typename Cx<R>::T;
     constexpr bool is64 = sizeof(R) == 8;
     constexpr int LOGE = is64 ? kLogRowsC128 : kLogRowsC64;
-    const DeviceSchedule &ds = is64 ? p->c128 : p->c64;
+    const DeviceSchedule &ds = p->sched;
     const uint32_t S = kLogThreads + LOGE;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
     if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
@@ -531,7 +581,7 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
             }
         }
         const uint64_t tiles = p->dim >> S;
-        const size_t smem = 2 * (size_t(1) << S) * sizeof(C);
+        const size_t smem = tiled_smem_bytes<LOGE, R>();
         k_tiled<LOGE, R><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
             ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err);
     } else {
@@ -660,8 +710,7 @@ extern "C" int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (g_num_sms == 0) cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, p->device);
-    p->c128.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
-    p->c64.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC64, kLogThreads);
+    p->sched.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
     st = upload(p.get());
     if (st) return st;
     if (storage == TCP_STORAGE_EAGER) {
@@ -703,10 +752,10 @@ extern "C" int tcp_mvp_plan_info(const tcp_mvp_plan *plan, tcp_mvp_plan_info_t *
     info->device = plan->device;
     info->transition_count = plan->transitions;
     info->device_bytes = plan->dev_bytes;
-    info->tile_bits_c128 = plan->c128.host.tile_bits;
-    info->tile_bits_c64 = plan->c64.host.tile_bits;
-    info->steps_c128 = plan->c128.host.step_d.size();
-    info->steps_c64 = plan->c64.host.step_d.size();
+    info->tile_bits = plan->sched.host.tile_bits;
+    info->log_threads = plan->sched.host.log_threads;
+    info->steps = plan->sched.host.step_info.size() / 4;
+    info->outer_patterns = plan->sched.host.distinct_outer;
     return TCP_OK;
 }
 
@@ -761,12 +810,12 @@ extern "C" int tcp_mvp_transition_count(const tcp_mvp_plan *plan, uint64_t *out_
         return fail(TCP_ERR_ALLOCATION, "device allocation of the transition counter failed");
     }
     cudaMemset(d_count, 0, sizeof(unsigned long long));
-    const uint32_t ngroups = static_cast<uint32_t>(plan->c128.host.g_mask.size());
+    const uint32_t ngroups = static_cast<uint32_t>(plan->sched.host.g_mask.size());
     const uint64_t total = static_cast<uint64_t>(ngroups) * plan->dim;
     if (total > 0) {
         const int threads = 256;
         uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 148ull * 64);
-        k_transitions<<<static_cast<unsigned>(blocks), threads>>>(plan->c128.dev, ngroups, plan->dim, d_count);
+        k_transitions<<<static_cast<unsigned>(blocks), threads>>>(plan->sched.dev, ngroups, plan->dim, d_count);
     }
     unsigned long long h = 0;
     e = cudaMemcpy(&h, d_count, sizeof h, cudaMemcpyDeviceToHost);
@@ -781,7 +830,7 @@ extern "C" int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, u
     if (st) return st;
     if (len != plan->dim) return length_error(plan->dim, len);
     if (d_diag == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
-    const tcp::Schedule &h = plan->c128.host;
+    const tcp::Schedule &h = plan->sched.host;
     uint32_t gzero = 0xffffffffu;
     for (size_t g = 0; g < h.g_mask.size(); ++g) {
         if (h.g_mask[g] == 0) {
@@ -792,7 +841,7 @@ extern "C" int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, u
     const int threads = 256;
     uint64_t blocks = std::min<uint64_t>((plan->dim + threads - 1) / threads, 1u << 20);
     k_diagonal<<<static_cast<unsigned>(blocks), threads, 0, static_cast<cudaStream_t>(stream)>>>(
-        plan->c128.dev, gzero, plan->dim, static_cast<double2 *>(d_diag));
+        plan->sched.dev, gzero, plan->dim, static_cast<double2 *>(d_diag));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "diagonal kernel launch");
 }
@@ -867,10 +916,10 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     if (e != cudaSuccess) return cuda_fail(e, "clearing the static scratch status");
     e = cudaMemcpyAsync(dx, state, bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "H2D copy into the static scratch");
-    const DeviceSchedule &ds = plan->c128;
+    const DeviceSchedule &ds = plan->sched;
     const uint32_t S = kTileBitsC128;
     if (plan->nqubits >= S && ds.host.tile_bits == S) {
-        const size_t smem = 2 * (size_t(1) << S) * sizeof(double2);
+        const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();
         k_tiled<kLogRowsC128, double><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(ds.dev, dx, dy,
                                                                                                   d_status);
     } else {

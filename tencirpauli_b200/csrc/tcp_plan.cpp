@@ -96,6 +96,13 @@ uint64_t distinct_x_masks(const std::vector<MatrixTerm> &terms) {
     return static_cast<uint64_t>(std::unique(m.begin(), m.end()) - m.begin());
 }
 
+namespace {
+template <typename T> void put(std::vector<uint8_t> &out, const T &v) {
+    const uint8_t *p = reinterpret_cast<const uint8_t *>(&v);
+    out.insert(out.end(), p, p + sizeof(T));
+}
+}  // namespace
+
 Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits,
                         uint32_t log_threads) {
     Schedule s;
@@ -104,8 +111,7 @@ Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, 
     const uint32_t S = s.tile_bits;
     const uint32_t L = s.log_threads;
     const uint64_t inner = (S >= 64) ? ~0ull : ((1ull << S) - 1);
-    const uint32_t jbits = S - L;
-    const uint32_t jcount = 1u << jbits;
+    const uint32_t jcount = 1u << (S - L);
     // (outer, inner, canonical index): a stable order that keeps canonical
     // term order inside every x-mask group.
     std::vector<uint64_t> order(terms.size());
@@ -115,59 +121,110 @@ Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, 
         if (da != db) return da < db;
         return (terms[a].x_mask & inner) < (terms[b].x_mask & inner);
     });
-    s.step_gbeg.push_back(0);
+    // group view
     s.g_tbeg.push_back(0);
     for (size_t i = 0; i < order.size(); ++i) {
         const MatrixTerm &t = terms[order[i]];
-        uint64_t d = t.x_mask >> S;
-        bool new_step = s.step_d.empty() || s.step_d.back() != d;
-        bool new_group = new_step || s.g_mask.back() != t.x_mask;
-        uint32_t tindex = static_cast<uint32_t>(s.t_z.size());
-        if (new_group) {
-            if (!s.g_mask.empty()) {
-                s.g_tbeg.push_back(tindex);
-                s.g_rec[s.g_rec.size() - 2] = tindex;  // end term of the previous group
-            }
-            if (new_step) {
-                if (!s.step_d.empty()) s.step_gbeg.push_back(static_cast<uint32_t>(s.g_mask.size()));
-                s.step_d.push_back(d);
-            }
+        if (s.g_mask.empty() || s.g_mask.back() != t.x_mask) {
+            if (!s.g_mask.empty()) s.g_tbeg.push_back(static_cast<uint32_t>(i));
             s.g_mask.push_back(t.x_mask);
-            s.g_rec.push_back(static_cast<uint32_t>(t.x_mask & inner));
-            s.g_rec.push_back(tindex);
-            s.g_rec.push_back(tindex);  // end, patched when the group closes
-            s.g_rec.push_back(0);
         }
-        // per-term record
-        const uint64_t zt = (S >= 64) ? 0 : (t.z_mask >> S);
-        const uint32_t zlo = static_cast<uint32_t>(t.z_mask & ((1ull << L) - 1));
-        const uint32_t zj = static_cast<uint32_t>((t.z_mask & inner) >> L);
-        uint32_t pattern = 0;
-        for (uint32_t jj = 0; jj < jcount; ++jj) pattern |= (static_cast<uint32_t>(__builtin_popcount(zj & jj)) & 1u) << jj;
-        uint32_t kind = (t.w_im == 0.0) ? kKindReal : ((t.w_re == 0.0) ? kKindImag : kKindComplex);
-        s.t_rec.push_back(static_cast<uint64_t>(zlo) | (static_cast<uint64_t>(pattern) << 32) |
-                          (static_cast<uint64_t>(kind) << 56));
-        s.t_rec.push_back(zt);
-        const bool flip = (__builtin_popcountll(zt & d) & 1) != 0;
-        const double wr = flip ? -t.w_re : t.w_re, wi = flip ? -t.w_im : t.w_im;
-        s.t_ws.push_back(wr);
-        s.t_ws.push_back(wi);
-        s.t_wfs.push_back(static_cast<float>(wr));
-        s.t_wfs.push_back(static_cast<float>(wi));
         s.t_z.push_back(t.z_mask);
         s.t_w.push_back(t.w_re);
         s.t_w.push_back(t.w_im);
         s.t_wf.push_back(static_cast<float>(t.w_re));
         s.t_wf.push_back(static_cast<float>(t.w_im));
     }
-    if (!s.g_mask.empty()) {
-        uint32_t tend = static_cast<uint32_t>(s.t_z.size());
-        s.g_tbeg.push_back(tend);
-        s.g_rec[s.g_rec.size() - 2] = tend;
-        s.step_gbeg.push_back(static_cast<uint32_t>(s.g_mask.size()));
-    } else {
-        s.g_tbeg.assign(1, 0);
-        s.step_gbeg.assign(1, 0);
+    if (!s.g_mask.empty()) s.g_tbeg.push_back(static_cast<uint32_t>(order.size()));
+
+    // step view: walk the groups, packing blocks of at most kBlockBytesMax
+    struct Pending {
+        uint32_t m_in;
+        size_t gid;                   // group index in the group view
+        std::vector<uint64_t> terms;  // indices into `terms`
+    };
+    uint64_t cur_d = 0;
+    std::vector<Pending> pend;
+    size_t pend_bytes = 0;
+    auto flush = [&]() {
+        if (pend.empty()) return;
+        const size_t off = s.blocks_c128.size();
+        uint32_t nterms = 0;
+        for (auto &g : pend) {
+            put(s.blocks_c128, g.m_in);
+            put(s.blocks_c128, nterms);
+            nterms += static_cast<uint32_t>(g.terms.size());
+            put(s.blocks_c128, nterms);
+            put(s.blocks_c128, uint32_t(0));
+        }
+        for (auto &g : pend) {
+            for (uint64_t ti : g.terms) {
+                const MatrixTerm &t = terms[ti];
+                const uint64_t zt = (S >= 64) ? 0 : (t.z_mask >> S);
+                const uint32_t zlo = static_cast<uint32_t>(t.z_mask & ((1ull << L) - 1));
+                const uint32_t zj = static_cast<uint32_t>((t.z_mask & inner) >> L);
+                uint32_t pattern = 0;
+                for (uint32_t jj = 0; jj < jcount; ++jj)
+                    pattern |= (static_cast<uint32_t>(__builtin_popcount(zj & jj)) & 1u) << jj;
+                const uint32_t kind = (t.w_im == 0.0) ? kKindReal : ((t.w_re == 0.0) ? kKindImag : kKindComplex);
+                const uint64_t zrec = static_cast<uint64_t>(zlo) | (static_cast<uint64_t>(pattern) << 32) |
+                                      (static_cast<uint64_t>(kind) << 56);
+                const bool flip = (__builtin_popcountll(zt & cur_d) & 1) != 0;
+                const double wr = flip ? -t.w_re : t.w_re, wi = flip ? -t.w_im : t.w_im;
+                put(s.blocks_c128, zrec);
+                put(s.blocks_c128, zt);
+                put(s.blocks_c128, wr);
+                put(s.blocks_c128, wi);
+            }
+        }
+        const size_t bytes = s.blocks_c128.size() - off;
+        s.step_info.push_back(static_cast<uint32_t>(cur_d));
+        s.step_info.push_back(static_cast<uint32_t>(cur_d >> 32));
+        s.step_info.push_back(static_cast<uint32_t>(off / 16));
+        s.step_info.push_back(static_cast<uint32_t>(pend.size()) | static_cast<uint32_t>((bytes / 16) << 16));
+        pend.clear();
+        pend_bytes = 0;
+    };
+    bool have_step = false;
+    for (size_t g = 0; g < s.g_mask.size(); ++g) {
+        const uint64_t d = s.g_mask[g] >> S;
+        const uint32_t m_in = static_cast<uint32_t>(s.g_mask[g] & inner);
+        if (!have_step || d != cur_d) {
+            flush();
+            cur_d = d;
+            have_step = true;
+            ++s.distinct_outer;
+        }
+        for (uint32_t t = s.g_tbeg[g]; t < s.g_tbeg[g + 1]; ++t) {
+            bool opens = pend.empty() || pend.back().gid != g;
+            if (pend_bytes + kTermRecBytes + (opens ? kGroupRecBytes : 0) > kBlockBytesMax) {
+                flush();
+                opens = true;
+            }
+            if (opens) {
+                pend.push_back(Pending{m_in, g, {}});
+                pend_bytes += kGroupRecBytes;
+            }
+            pend.back().terms.push_back(order[t]);
+            pend_bytes += kTermRecBytes;
+        }
+    }
+    flush();
+    // complex64 blocks: same layout, weights as two floats + 8 pad bytes
+    s.blocks_c64 = s.blocks_c128;
+    for (size_t i = 0; i + 4 <= s.step_info.size(); i += 4) {
+        const size_t off = static_cast<size_t>(s.step_info[i + 2]) * 16;
+        const uint32_t ng = s.step_info[i + 3] & 0xffffu;
+        const size_t bytes = static_cast<size_t>(s.step_info[i + 3] >> 16) * 16;
+        for (size_t p = off + ng * kGroupRecBytes; p < off + bytes; p += kTermRecBytes) {
+            double wr, wi;
+            std::memcpy(&wr, &s.blocks_c128[p + 16], 8);
+            std::memcpy(&wi, &s.blocks_c128[p + 24], 8);
+            const float fr = static_cast<float>(wr), fi = static_cast<float>(wi);
+            std::memcpy(&s.blocks_c64[p + 16], &fr, 4);
+            std::memcpy(&s.blocks_c64[p + 20], &fi, 4);
+            std::memset(&s.blocks_c64[p + 24], 0, 8);
+        }
     }
     return s;
 }
