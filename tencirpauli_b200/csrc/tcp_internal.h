@@ -37,11 +37,12 @@ struct MatrixTerm {
 // inner mask m the thread reads source rows (t ^ (m & (T-1))) + jj * T and row
 // j takes source jj = j ^ (m >> log_threads).  The sign of a term at source
 // column c = (tile ^ d) * 2^S + local is
-//   parity(zt & tile) ^ parity(zt & d) ^ parity(zlo & (t ^ m_lo)) ^ parity(zj & jj)
-// with zt = z >> S, zlo = z & (T-1), zj = (z & (2^S-1)) >> log_threads.  The
-// schedule folds parity(zt & d) into the term's weight, stores the 2^(S-logT)
-// bit pattern parity(zj & jj) per term, and leaves the two per-thread parities
-// to the kernel.
+//   parity(zt & tile) ^ parity(zt & d) ^ parity(zlo & t) ^ parity(zlo & m_lo) ^ parity(zj & jj)
+// with zt = z >> S, zlo = z & (T-1), m_lo = m & (T-1),
+// zj = (z & (2^S-1)) >> log_threads.  The schedule folds parity(zt & d) and
+// parity(zlo & m_lo) into the term's weight and stores the 2^(S-logT)-bit
+// pattern parity(zj & jj); the kernel applies parity(zt & tile) once per step
+// and tile, and parity(zlo & t) per thread.
 struct Schedule {
     uint32_t tile_bits = 0;
     uint32_t log_threads = 0;

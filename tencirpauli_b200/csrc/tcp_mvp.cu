@@ -39,6 +39,7 @@ constexpr int kLogRowsC128 = 3;              // 8 rows per thread  -> 4096-row t
 constexpr int kLogRowsC64 = 3;               // 8 rows per thread  -> 4096-row tile
 constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
+constexpr uint32_t kCompensateGroups = 4;   // FP32: groups per Kahan fold
 
 // Error bits written by kernels into the plan's device status word.
 constexpr int kErrTimeout = 1;
@@ -148,14 +149,14 @@ __device__ __forceinline__ float flip_by(float w, uint32_t odd) {
 }
 
 // Accumulator of one output row.  FP64: terms are added straight into the
-// row sum.  FP32: a group's terms are summed into a temporary, and the group's
-// total is added to the row sum with Kahan compensation (one compensation
-// term per component, carried across x-mask groups).
+// row sum.  FP32: terms are summed into a running partial sum, which is folded
+// into the row sum with Kahan compensation (one compensation term per
+// component) after every kCompensateGroups x-mask groups and at the end of
+// every step, so the long sum across x-mask groups is compensated.
 template <typename R> struct Acc;
 template <> struct Acc<double> {
     double re = 0.0, im = 0.0;
-    __device__ __forceinline__ void begin_group() {}
-    __device__ __forceinline__ void end_group() {}
+    __device__ __forceinline__ void compensate() {}
     __device__ __forceinline__ void add_real(double w, double2 v) {
         re = fma(w, v.x, re);
         im = fma(w, v.y, im);
@@ -183,10 +184,11 @@ template <> struct Acc<float> {
         comp = __fsub_rn(__fsub_rn(tv, sum), yv);
         sum = tv;
     }
-    __device__ __forceinline__ void begin_group() { pre = pim = 0.f; }
-    __device__ __forceinline__ void end_group() {
+    // Fold the running partial sum into the Kahan-compensated row sum.
+    __device__ __forceinline__ void compensate() {
         kahan(re, cre, pre);
         kahan(im, cim, pim);
+        pre = pim = 0.f;
     }
     __device__ __forceinline__ void add_real(float w, float2 v) {
         pre = __fmaf_rn(w, v.x, pre);
@@ -203,67 +205,97 @@ template <> struct Acc<float> {
         pim = __fmaf_rn(wi, v.x, pim);
     }
     __device__ __forceinline__ void add_product(float dre, float dim, float2 v) {
-        begin_group();
         add_complex(dre, dim, v);
-        end_group();
+        compensate();
     }
     __device__ __forceinline__ float2 value() const { return make_float2(re, im); }
 };
 
 // --------------------------------- kernels ---------------------------------
+// One term applied to the thread's E rows.  `rec` is the term record's first
+// 16 bytes (zlo | (pattern | kind << 24) << 32, zt); `w` its weight with the
+// per-step and per-group signs already folded in.  The remaining sign,
+// parity(zlo & tid) ^ parity(zt & tile), is one POPC of an XOR (the parity of
+// a XOR equals the XOR of the parities).
+template <int JH, int LOGE, typename R>
+__device__ __forceinline__ void apply_term(ulonglong2 rec, typename Cx<R>::T w, uint32_t tid, uint64_t tile,
+                                           const typename Cx<R>::T (&xv)[1 << LOGE], Acc<R> (&acc)[1 << LOGE]) {
+    constexpr int E = 1 << LOGE;
+    constexpr uint32_t kPatMask = (1u << E) - 1u;
+    const uint32_t lo = static_cast<uint32_t>(rec.x);
+    const uint32_t hi = static_cast<uint32_t>(rec.x >> 32);
+    const uint64_t zt_tile = rec.y & tile;
+    const uint32_t base =
+        __popc((lo & tid) ^ static_cast<uint32_t>(zt_tile) ^ static_cast<uint32_t>(zt_tile >> 32)) & 1u;
+    const uint32_t pattern = hi & kPatMask;
+    const uint32_t kind = hi >> 24;
+    if (pattern == 0u) {
+        const R wr = flip_by(w.x, base), wi = flip_by(w.y, base);
+        if (kind == tcp::kKindReal) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(wr, xv[jj]);
+        } else if (kind == tcp::kKindImag) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(wi, xv[jj]);
+        } else {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_complex(wr, wi, xv[jj]);
+        }
+    } else {
+        const uint32_t pat = (pattern ^ (0u - base)) & kPatMask;  // sign bit of every source jj
+        if (kind == tcp::kKindReal) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(flip_if(w.x, pat, jj), xv[jj]);
+        } else if (kind == tcp::kKindImag) {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(flip_if(w.y, pat, jj), xv[jj]);
+        } else {
+#pragma unroll
+            for (int jj = 0; jj < E; ++jj)
+                acc[jj ^ JH].add_complex(flip_if(w.x, pat, jj), flip_if(w.y, pat, jj), xv[jj]);
+        }
+    }
+}
+
 // Terms of one x-mask group applied to the thread's E rows.  JH (the group's
 // inner-mask bits above the thread index) is a template parameter, so row j
 // reads the loaded source value jj = j ^ JH at a compile-time register index.
-// Term records come from the step block in shared memory.  A term whose z mask
+// Term records come from the step block in shared memory; a term whose z mask
 // has no bit among the thread's row bits (pattern 0) has one sign for all E
-// rows; otherwise the sign of source jj is bit jj of the pattern.
+// rows, otherwise the sign of source jj is bit jj of the pattern.
 template <int JH, int LOGE, typename R>
 __device__ __forceinline__ void apply_group(const unsigned char *__restrict__ trm, uint32_t tb, uint32_t te,
-                                            uint32_t tl, uint64_t tile, const typename Cx<R>::T (&xv)[1 << LOGE],
+                                            uint32_t tid, uint64_t tile, const typename Cx<R>::T (&xv)[1 << LOGE],
                                             Acc<R> (&acc)[1 << LOGE]) {
-    using C = typename Cx<R>::T;
-    constexpr int E = 1 << LOGE;
-    constexpr uint32_t kPatMask = (1u << E) - 1u;
-#pragma unroll
-    for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].begin_group();
     for (uint32_t t = tb; t < te; ++t) {
-        const unsigned char *rp = trm + t * tcp::kTermRecBytes;
-        const ulonglong2 rec = *reinterpret_cast<const ulonglong2 *>(rp);
-        const C w = record_weight<R>(rp);
-        const uint32_t zlo = static_cast<uint32_t>(rec.x);
-        const uint32_t hi = static_cast<uint32_t>(rec.x >> 32);
-        const uint32_t base = (__popc(zlo & tl) + __popcll(rec.y & tile)) & 1u;
-        const uint32_t pattern = hi & kPatMask;
-        const uint32_t kind = hi >> 24;
-        if (pattern == 0u) {
-            const R wr = flip_by(w.x, base), wi = flip_by(w.y, base);
-            if (kind == tcp::kKindReal) {
-#pragma unroll
-                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(wr, xv[jj]);
-            } else if (kind == tcp::kKindImag) {
-#pragma unroll
-                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(wi, xv[jj]);
-            } else {
-#pragma unroll
-                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_complex(wr, wi, xv[jj]);
-            }
-        } else {
-            const uint32_t pat = (pattern ^ (0u - base)) & kPatMask;  // sign bit of every source jj
-            if (kind == tcp::kKindReal) {
-#pragma unroll
-                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_real(flip_if(w.x, pat, jj), xv[jj]);
-            } else if (kind == tcp::kKindImag) {
-#pragma unroll
-                for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].add_imag(flip_if(w.y, pat, jj), xv[jj]);
-            } else {
-#pragma unroll
-                for (int jj = 0; jj < E; ++jj)
-                    acc[jj ^ JH].add_complex(flip_if(w.x, pat, jj), flip_if(w.y, pat, jj), xv[jj]);
-            }
-        }
+        const unsigned char *r0 = trm + t * tcp::kTermRecBytes;
+        apply_term<JH, LOGE, R>(*reinterpret_cast<const ulonglong2 *>(r0), record_weight<R>(r0), tid, tile, xv, acc);
     }
+}
+
+// Dispatch a group on its inner-mask bits above the thread index.
+template <int LOGE, typename R>
+__device__ __forceinline__ void dispatch_group(uint32_t jh, const unsigned char *__restrict__ trm, uint32_t tb,
+                                               uint32_t te, uint32_t tid, uint64_t tile,
+                                               const typename Cx<R>::T (&xv)[1 << LOGE], Acc<R> (&acc)[1 << LOGE]) {
+    switch (jh) {
+    case 0: apply_group<0, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    case 1: apply_group<1, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    case 2: apply_group<2, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    case 3: apply_group<3, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    case 4: apply_group<4, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    case 5: apply_group<5, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    case 6: apply_group<6, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    default: apply_group<7, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
+    }
+}
+
+// Source values of one group for the thread: xv[jj] = tile[(tid ^ m_lo) + jj * T].
+template <int LOGE, typename C>
+__device__ __forceinline__ void load_group(const C *__restrict__ xs, uint32_t tid, uint32_t m, C (&xv)[1 << LOGE]) {
+    const C *src = xs + (tid ^ (m & (kThreads - 1)));
 #pragma unroll
-    for (int jj = 0; jj < E; ++jj) acc[jj ^ JH].end_group();
+    for (int jj = 0; jj < (1 << LOGE); ++jj) xv[jj] = src[jj << kLogThreads];
 }
 
 template <typename R> __device__ __forceinline__ const unsigned char *step_blocks(const DevSchedule &s);
@@ -339,21 +371,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         const unsigned char *trm = blk + ng * tcp::kGroupRecBytes;
         for (uint32_t g = 0; g < ng; ++g) {
             const uint4 gr = grp[g];
-            const uint32_t tl = tid ^ (gr.x & (kThreads - 1));
-            const uint32_t jh = gr.x >> kLogThreads;
             C xv[E];
-            const C *src = xs + tl;
+            load_group<LOGE>(xs, tid, gr.x, xv);
+            dispatch_group<LOGE, R>(gr.x >> kLogThreads, trm, gr.y, gr.z, tid, tile, xv, acc);
+            // FP32: fold the running group sum into the compensated row sum
+            // every kCompensateGroups groups and at the end of the step.
+            if (((g + 1) % kCompensateGroups) == 0u || g + 1 == ng) {
 #pragma unroll
-            for (int jj = 0; jj < E; ++jj) xv[jj] = src[jj << kLogThreads];
-            switch (jh) {
-            case 0: apply_group<0, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 1: apply_group<1, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 2: apply_group<2, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 3: apply_group<3, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 4: apply_group<4, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 5: apply_group<5, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            case 6: apply_group<6, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
-            default: apply_group<7, LOGE, R>(trm, gr.y, gr.z, tl, tile, xv, acc); break;
+                for (int j = 0; j < E; ++j) acc[j].compensate();
             }
         }
     }
