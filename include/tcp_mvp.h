@@ -154,6 +154,36 @@ int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, voi
                               uint64_t len, uint32_t nrhs, int dtype, void *stream);
 
 /*
+ * Batched MVP: many plans (Hamiltonians of uneven qubit and term counts), each
+ * applied to a block of `nrhs` right-hand sides, in one persistent kernel
+ * launch replayed from a CUDA graph.  No counterpart in the reference (its
+ * MvpPlan::apply_into, hamiltonian.rs:204-270, takes one state per call);
+ * per vector the arithmetic is that of tcp_mvp_apply_into_device.
+ * Buffers: d_x[h] / d_y[h] hold member h's nrhs vectors, RHS-major (vector v at
+ * offset v * 2^n_h), complex128 or complex64 per `dtype`, 16-byte aligned.
+ * Every member needs at least 8 qubits.  The batch keeps pointers to its plans,
+ * which must outlive it.  Work items are (member, tile of 2^tile_rows_log2
+ * rows, block of rhs_block vectors), largest member first.
+ */
+typedef struct tcp_mvp_batch tcp_mvp_batch;
+int tcp_mvp_batch_create(uint32_t count, const tcp_mvp_plan *const *plans, uint32_t nrhs, int dtype,
+                         tcp_mvp_batch **out_batch);
+int tcp_mvp_batch_destroy(tcp_mvp_batch *batch);
+/* Choose the tile rows (2^8..2^10) and RHS block (1, 2, 4, 8; divides nrhs). */
+int tcp_mvp_batch_configure(tcp_mvp_batch *batch, uint32_t tile_rows_log2, uint32_t rhs_block);
+/* Time every kernel variant on these buffers (`repeats` launches each) and keep
+ * the fastest; with a non-empty cache_path the choice is read from / appended
+ * to that file, keyed by device, dtype, nrhs and every member's (n, T, G). */
+int tcp_mvp_batch_autotune(tcp_mvp_batch *batch, const void *const *d_x, void *const *d_y,
+                           const char *cache_path, uint32_t repeats, void *stream);
+/* y_h = H_h x_h for every member; asynchronous on `stream` (graph launch). */
+int tcp_mvp_batch_apply(tcp_mvp_batch *batch, const void *const *d_x, void *const *d_y, void *stream);
+int tcp_mvp_batch_info(const tcp_mvp_batch *batch, uint32_t *tile_rows_log2, uint32_t *rhs_block,
+                       uint64_t *items, uint32_t *grid);
+/* Synchronise and report (then clear) a device-side error of the batch. */
+int tcp_mvp_batch_device_status(tcp_mvp_batch *batch);
+
+/*
  * Allocation-free host apply.  This entry point has no counterpart in the
  * reference; it exists for callers that must not allocate device memory while
  * they apply, such as applications whose own allocator owns the GPU's memory

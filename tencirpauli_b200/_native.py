@@ -59,6 +59,13 @@ EXPORTED_SYMBOLS = (
     "tcp_mvp_plan_device_status",
     "tcp_mvp_transition_count",
     "tcp_mvp_diagonal_device",
+    "tcp_mvp_batch_create",
+    "tcp_mvp_batch_destroy",
+    "tcp_mvp_batch_configure",
+    "tcp_mvp_batch_autotune",
+    "tcp_mvp_batch_apply",
+    "tcp_mvp_batch_info",
+    "tcp_mvp_batch_device_status",
 )
 
 
@@ -118,6 +125,14 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mvp_plan_device_status.argtypes = [vp]
         lib.tcp_mvp_transition_count.argtypes = [vp, u64p]
         lib.tcp_mvp_diagonal_device.argtypes = [vp, vp, u64, vp]
+        vpp = ctypes.POINTER(vp)
+        lib.tcp_mvp_batch_create.argtypes = [u32, vpp, u32, i32, vpp]
+        lib.tcp_mvp_batch_destroy.argtypes = [vp]
+        lib.tcp_mvp_batch_configure.argtypes = [vp, u32, u32]
+        lib.tcp_mvp_batch_autotune.argtypes = [vp, vpp, vpp, ctypes.c_char_p, u32, vp]
+        lib.tcp_mvp_batch_apply.argtypes = [vp, vpp, vpp, vp]
+        lib.tcp_mvp_batch_info.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(u32), ctypes.POINTER(u64), ctypes.POINTER(u32)]
+        lib.tcp_mvp_batch_device_status.argtypes = [vp]
         for name in EXPORTED_SYMBOLS:
             if name not in ("tcp_last_error",):
                 getattr(lib, name).restype = i32

@@ -1,0 +1,194 @@
+// Device-side building blocks shared by the MVP kernels of libtcpmvp.so:
+// launch constants, the device view of a plan's schedule, PTX wrappers for
+// the TMA bulk-copy engine and mbarriers (with bounded waits), complex types,
+// sign helpers and the row accumulators.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tcp_internal.h"
+
+namespace tcpdev {
+
+constexpr int kLogThreads = 9;               // 512 threads per CTA
+constexpr int kThreads = 1 << kLogThreads;
+constexpr int kLogRowsC128 = 3;              // 8 rows per thread  -> 4096-row tile
+constexpr int kLogRowsC64 = 3;               // 8 rows per thread  -> 4096-row tile
+constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
+constexpr uint32_t kCompensateGroups = 4;   // FP32: groups per Kahan fold
+
+// Error bits written by kernels into the plan's device status word.
+constexpr int kErrTimeout = 1;
+
+struct DevSchedule {
+    // step view (tiled kernels); see tcp::Schedule
+    const uint4 *step_info;          // d lo, d hi, block offset / 16, ngroups | (bytes / 16) << 16
+    const unsigned char *blocks128;  // step blocks with FP64 weights
+    const unsigned char *blocks64;   // step blocks with FP32 weights
+    uint32_t nsteps;
+    uint32_t tile_bits;
+    // group view (row kernel, transition count, diagonal): unfolded weights
+    const uint64_t *g_mask;
+    const uint32_t *g_tbeg;
+    const uint64_t *t_z;
+    const double2 *t_w;
+    const float2 *t_wf;
+    uint32_t ngroups;
+};
+
+// ------------------------------- PTX helpers -------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// 1-D bulk copy global -> shared through the TMA engine; completes tx bytes
+// on the mbarrier.  Both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait on an mbarrier phase: returns false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long start = global_ns();
+    for (uint32_t spin = 1;; ++spin) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((spin & 255u) == 0u && global_ns() - start > kWaitLimitNs) return false;
+    }
+}
+
+// ------------------------------ complex types ------------------------------
+template <typename R> struct Cx;
+template <> struct Cx<double> { using T = double2; };
+template <> struct Cx<float> { using T = float2; };
+
+template <typename R> __device__ __forceinline__ typename Cx<R>::T weight_of(const DevSchedule &s, uint32_t t);
+template <> __device__ __forceinline__ double2 weight_of<double>(const DevSchedule &s, uint32_t t) {
+    return __ldg(&s.t_w[t]);
+}
+template <> __device__ __forceinline__ float2 weight_of<float>(const DevSchedule &s, uint32_t t) {
+    return __ldg(&s.t_wf[t]);
+}
+// Weight of a term record in a shared-memory step block (offset 16 bytes).
+template <typename R> __device__ __forceinline__ typename Cx<R>::T record_weight(const unsigned char *rec);
+template <> __device__ __forceinline__ double2 record_weight<double>(const unsigned char *rec) {
+    return *reinterpret_cast<const double2 *>(rec + 16);
+}
+template <> __device__ __forceinline__ float2 record_weight<float>(const unsigned char *rec) {
+    return *reinterpret_cast<const float2 *>(rec + 16);
+}
+
+// Flip the sign of w when bit `bit` of `pattern` is set (an integer op on the
+// sign bit; `bit` is a compile-time constant after unrolling).
+__device__ __forceinline__ double flip_if(double w, uint32_t pattern, int bit) {
+    const int hi = __double2hiint(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u);
+    return __hiloint2double(hi, __double2loint(w));
+}
+__device__ __forceinline__ float flip_if(float w, uint32_t pattern, int bit) {
+    return __int_as_float(__float_as_int(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u));
+}
+// Flip the sign of w when `odd` (0 or 1) is set.
+__device__ __forceinline__ double flip_by(double w, uint32_t odd) {
+    return __hiloint2double(__double2hiint(w) ^ static_cast<int>(odd << 31), __double2loint(w));
+}
+__device__ __forceinline__ float flip_by(float w, uint32_t odd) {
+    return __int_as_float(__float_as_int(w) ^ static_cast<int>(odd << 31));
+}
+
+// Accumulator of one output row.  FP64: terms are added straight into the
+// row sum.  FP32: terms are summed into a running partial sum, which is folded
+// into the row sum with Kahan compensation (one compensation term per
+// component) after every kCompensateGroups x-mask groups and at the end of
+// every step, so the long sum across x-mask groups is compensated.
+template <typename R> struct Acc;
+template <> struct Acc<double> {
+    double re = 0.0, im = 0.0;
+    __device__ __forceinline__ void compensate() {}
+    __device__ __forceinline__ void add_real(double w, double2 v) {
+        re = fma(w, v.x, re);
+        im = fma(w, v.y, im);
+    }
+    __device__ __forceinline__ void add_imag(double w, double2 v) {
+        re = fma(-w, v.y, re);
+        im = fma(w, v.x, im);
+    }
+    __device__ __forceinline__ void add_complex(double wr, double wi, double2 v) {
+        re = fma(wr, v.x, re);
+        re = fma(-wi, v.y, re);
+        im = fma(wr, v.y, im);
+        im = fma(wi, v.x, im);
+    }
+    // group view: D = sum of signed weights, then y += D x
+    __device__ __forceinline__ void add_product(double dre, double dim, double2 v) { add_complex(dre, dim, v); }
+    __device__ __forceinline__ double2 value() const { return make_double2(re, im); }
+};
+template <> struct Acc<float> {
+    float re = 0.f, im = 0.f, cre = 0.f, cim = 0.f;  // Kahan sums
+    float pre = 0.f, pim = 0.f;                      // current group's contribution
+    __device__ __forceinline__ static void kahan(float &sum, float &comp, float term) {
+        const float yv = __fsub_rn(term, comp);
+        const float tv = __fadd_rn(sum, yv);
+        comp = __fsub_rn(__fsub_rn(tv, sum), yv);
+        sum = tv;
+    }
+    // Fold the running partial sum into the Kahan-compensated row sum.
+    __device__ __forceinline__ void compensate() {
+        kahan(re, cre, pre);
+        kahan(im, cim, pim);
+        pre = pim = 0.f;
+    }
+    __device__ __forceinline__ void add_real(float w, float2 v) {
+        pre = __fmaf_rn(w, v.x, pre);
+        pim = __fmaf_rn(w, v.y, pim);
+    }
+    __device__ __forceinline__ void add_imag(float w, float2 v) {
+        pre = __fmaf_rn(-w, v.y, pre);
+        pim = __fmaf_rn(w, v.x, pim);
+    }
+    __device__ __forceinline__ void add_complex(float wr, float wi, float2 v) {
+        pre = __fmaf_rn(wr, v.x, pre);
+        pre = __fmaf_rn(-wi, v.y, pre);
+        pim = __fmaf_rn(wr, v.y, pim);
+        pim = __fmaf_rn(wi, v.x, pim);
+    }
+    __device__ __forceinline__ void add_product(float dre, float dim, float2 v) {
+        add_complex(dre, dim, v);
+        compensate();
+    }
+    __device__ __forceinline__ float2 value() const { return make_float2(re, im); }
+};
+
+
+}  // namespace tcpdev

@@ -31,185 +31,12 @@
 
 using tcp::fail;
 
+#include "tcp_device.cuh"
+#include "tcp_plan_impl.h"
+
+using namespace tcpdev;
+
 namespace {
-
-constexpr int kLogThreads = 9;               // 512 threads per CTA
-constexpr int kThreads = 1 << kLogThreads;
-constexpr int kLogRowsC128 = 3;              // 8 rows per thread  -> 4096-row tile
-constexpr int kLogRowsC64 = 3;               // 8 rows per thread  -> 4096-row tile
-constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
-constexpr uint32_t kCompensateGroups = 4;   // FP32: groups per Kahan fold
-
-// Error bits written by kernels into the plan's device status word.
-constexpr int kErrTimeout = 1;
-
-struct DevSchedule {
-    // step view (tiled kernels); see tcp::Schedule
-    const uint4 *step_info;          // d lo, d hi, block offset / 16, ngroups | (bytes / 16) << 16
-    const unsigned char *blocks128;  // step blocks with FP64 weights
-    const unsigned char *blocks64;   // step blocks with FP32 weights
-    uint32_t nsteps;
-    uint32_t tile_bits;
-    // group view (row kernel, transition count, diagonal): unfolded weights
-    const uint64_t *g_mask;
-    const uint32_t *g_tbeg;
-    const uint64_t *t_z;
-    const double2 *t_w;
-    const float2 *t_wf;
-    uint32_t ngroups;
-};
-
-// ------------------------------- PTX helpers -------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-// 1-D bulk copy global -> shared through the TMA engine; completes tx bytes
-// on the mbarrier.  Both addresses 16-byte aligned, size a multiple of 16.
-__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok;
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Bounded wait on an mbarrier phase: returns false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long start = global_ns();
-    for (uint32_t spin = 1;; ++spin) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((spin & 255u) == 0u && global_ns() - start > kWaitLimitNs) return false;
-    }
-}
-
-// ------------------------------ complex types ------------------------------
-template <typename R> struct Cx;
-template <> struct Cx<double> { using T = double2; };
-template <> struct Cx<float> { using T = float2; };
-
-template <typename R> __device__ __forceinline__ typename Cx<R>::T weight_of(const DevSchedule &s, uint32_t t);
-template <> __device__ __forceinline__ double2 weight_of<double>(const DevSchedule &s, uint32_t t) {
-    return __ldg(&s.t_w[t]);
-}
-template <> __device__ __forceinline__ float2 weight_of<float>(const DevSchedule &s, uint32_t t) {
-    return __ldg(&s.t_wf[t]);
-}
-// Weight of a term record in a shared-memory step block (offset 16 bytes).
-template <typename R> __device__ __forceinline__ typename Cx<R>::T record_weight(const unsigned char *rec);
-template <> __device__ __forceinline__ double2 record_weight<double>(const unsigned char *rec) {
-    return *reinterpret_cast<const double2 *>(rec + 16);
-}
-template <> __device__ __forceinline__ float2 record_weight<float>(const unsigned char *rec) {
-    return *reinterpret_cast<const float2 *>(rec + 16);
-}
-
-// Flip the sign of w when bit `bit` of `pattern` is set (an integer op on the
-// sign bit; `bit` is a compile-time constant after unrolling).
-__device__ __forceinline__ double flip_if(double w, uint32_t pattern, int bit) {
-    const int hi = __double2hiint(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u);
-    return __hiloint2double(hi, __double2loint(w));
-}
-__device__ __forceinline__ float flip_if(float w, uint32_t pattern, int bit) {
-    return __int_as_float(__float_as_int(w) ^ static_cast<int>((pattern << (31 - bit)) & 0x80000000u));
-}
-// Flip the sign of w when `odd` (0 or 1) is set.
-__device__ __forceinline__ double flip_by(double w, uint32_t odd) {
-    return __hiloint2double(__double2hiint(w) ^ static_cast<int>(odd << 31), __double2loint(w));
-}
-__device__ __forceinline__ float flip_by(float w, uint32_t odd) {
-    return __int_as_float(__float_as_int(w) ^ static_cast<int>(odd << 31));
-}
-
-// Accumulator of one output row.  FP64: terms are added straight into the
-// row sum.  FP32: terms are summed into a running partial sum, which is folded
-// into the row sum with Kahan compensation (one compensation term per
-// component) after every kCompensateGroups x-mask groups and at the end of
-// every step, so the long sum across x-mask groups is compensated.
-template <typename R> struct Acc;
-template <> struct Acc<double> {
-    double re = 0.0, im = 0.0;
-    __device__ __forceinline__ void compensate() {}
-    __device__ __forceinline__ void add_real(double w, double2 v) {
-        re = fma(w, v.x, re);
-        im = fma(w, v.y, im);
-    }
-    __device__ __forceinline__ void add_imag(double w, double2 v) {
-        re = fma(-w, v.y, re);
-        im = fma(w, v.x, im);
-    }
-    __device__ __forceinline__ void add_complex(double wr, double wi, double2 v) {
-        re = fma(wr, v.x, re);
-        re = fma(-wi, v.y, re);
-        im = fma(wr, v.y, im);
-        im = fma(wi, v.x, im);
-    }
-    // group view: D = sum of signed weights, then y += D x
-    __device__ __forceinline__ void add_product(double dre, double dim, double2 v) { add_complex(dre, dim, v); }
-    __device__ __forceinline__ double2 value() const { return make_double2(re, im); }
-};
-template <> struct Acc<float> {
-    float re = 0.f, im = 0.f, cre = 0.f, cim = 0.f;  // Kahan sums
-    float pre = 0.f, pim = 0.f;                      // current group's contribution
-    __device__ __forceinline__ static void kahan(float &sum, float &comp, float term) {
-        const float yv = __fsub_rn(term, comp);
-        const float tv = __fadd_rn(sum, yv);
-        comp = __fsub_rn(__fsub_rn(tv, sum), yv);
-        sum = tv;
-    }
-    // Fold the running partial sum into the Kahan-compensated row sum.
-    __device__ __forceinline__ void compensate() {
-        kahan(re, cre, pre);
-        kahan(im, cim, pim);
-        pre = pim = 0.f;
-    }
-    __device__ __forceinline__ void add_real(float w, float2 v) {
-        pre = __fmaf_rn(w, v.x, pre);
-        pim = __fmaf_rn(w, v.y, pim);
-    }
-    __device__ __forceinline__ void add_imag(float w, float2 v) {
-        pre = __fmaf_rn(-w, v.y, pre);
-        pim = __fmaf_rn(w, v.x, pim);
-    }
-    __device__ __forceinline__ void add_complex(float wr, float wi, float2 v) {
-        pre = __fmaf_rn(wr, v.x, pre);
-        pre = __fmaf_rn(-wi, v.y, pre);
-        pim = __fmaf_rn(wr, v.y, pim);
-        pim = __fmaf_rn(wi, v.x, pim);
-    }
-    __device__ __forceinline__ void add_product(float dre, float dim, float2 v) {
-        add_complex(dre, dim, v);
-        compensate();
-    }
-    __device__ __forceinline__ float2 value() const { return make_float2(re, im); }
-};
 
 // --------------------------------- kernels ---------------------------------
 // One term applied to the thread's E rows.  `rec` is the term record's first
@@ -450,53 +277,56 @@ __global__ void k_diagonal(DevSchedule s, uint32_t gzero, uint64_t dim, double2 
     }
 }
 
+}  // namespace
+
 // --------------------------------- host side --------------------------------
+namespace tcp {
+
 int cuda_fail(cudaError_t e, const char *what) {
     return fail(TCP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
 cudaError_t dev_malloc(void **p, size_t bytes) {
-    if (tcp::injected_alloc_failure()) {
+    if (injected_alloc_failure()) {
         *p = nullptr;
         return cudaErrorMemoryAllocation;
     }
     return cudaMalloc(p, bytes);
 }
 
-struct DeviceSchedule {
-    tcp::Schedule host;
-    DevSchedule dev{};
-};
 
-struct Workspace {
-    void *x = nullptr;
-    void *y = nullptr;
-    size_t bytes = 0;
-};
+int check_plan(const tcp_mvp_plan *plan) {
+    if (plan == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "plan is null");
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev != plan->device) {
+        return fail(TCP_ERR_WRONG_DEVICE, "plan lives on device " + std::to_string(plan->device) +
+                                              " but the current device is " + std::to_string(dev));
+    }
+    return TCP_OK;
+}
 
-int g_num_sms = 0;
+int length_error(uint64_t expected, uint64_t actual) {
+    return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH,
+                "expected structure length " + std::to_string(expected) + ", got " + std::to_string(actual));
+}
 
-}  // namespace
+bool overlaps(const void *a, const void *b, size_t bytes) {
+    auto pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    return pa < pb + bytes && pb < pa + bytes;
+}
+}  // namespace tcp
 
-struct tcp_mvp_plan {
-    uint32_t nqubits = 0;
-    uint32_t word_count = 0;
-    uint64_t dim = 0;
-    int storage = 0;
-    int device = 0;
-    int64_t transitions = -1;
-    std::vector<tcp::MatrixTerm> terms;
-    uint64_t group_count = 0;
-    DeviceSchedule sched;  // one schedule (4096-row tiles) serves both precisions
-    void *dev_block = nullptr;
-    size_t dev_bytes = 0;
-    int *d_err = nullptr;
-    mutable std::mutex ws_mutex;
-    mutable std::vector<Workspace> ws_free;
-    mutable std::vector<Workspace> ws_all;
-};
+using tcp::check_plan;
+using tcp::cuda_fail;
+using tcp::dev_malloc;
+using tcp::length_error;
+using tcp::overlaps;
 
 namespace {
+
+int g_num_sms = 0;
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -510,7 +340,7 @@ int upload(tcp_mvp_plan *p) {
     std::vector<Piece> pieces;
     auto add = [&](const void *src, size_t bytes, const void **dst) { pieces.push_back({src, bytes, dst}); };
     {
-        DeviceSchedule *ds = &p->sched;
+        tcp::DeviceSchedule *ds = &p->sched;
         tcp::Schedule &h = ds->host;
         add(h.step_info.data(), h.step_info.size() * 4, reinterpret_cast<const void **>(&ds->dev.step_info));
         add(h.blocks_c128.data(), h.blocks_c128.size(), reinterpret_cast<const void **>(&ds->dev.blocks128));
@@ -551,27 +381,8 @@ int upload(tcp_mvp_plan *p) {
     return TCP_OK;
 }
 
-int check_plan(const tcp_mvp_plan *plan) {
-    if (plan == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "plan is null");
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev != plan->device) {
-        return fail(TCP_ERR_WRONG_DEVICE, "plan lives on device " + std::to_string(plan->device) +
-                                              " but the current device is " + std::to_string(dev));
-    }
-    return TCP_OK;
-}
 
-int length_error(uint64_t expected, uint64_t actual) {
-    return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH,
-                "expected structure length " + std::to_string(expected) + ", got " + std::to_string(actual));
-}
 
-bool overlaps(const void *a, const void *b, size_t bytes) {
-    auto pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
-    return pa < pb + bytes && pb < pa + bytes;
-}
 
 template <int LOGE, typename R> constexpr size_t tiled_smem_bytes() {
     return 2 * (size_t(1) << (kLogThreads + LOGE)) * sizeof(typename Cx<R>::T) + 2 * size_t(tcp::kBlockBytesMax);
@@ -590,7 +401,7 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
     using C = typename Cx<R>::T;
     constexpr bool is64 = sizeof(R) == 8;
     constexpr int LOGE = is64 ? kLogRowsC128 : kLogRowsC64;
-    const DeviceSchedule &ds = p->sched;
+    const tcp::DeviceSchedule &ds = p->sched;
     const uint32_t S = kLogThreads + LOGE;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
     if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
@@ -641,7 +452,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     if (state == nullptr || result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     const size_t bytes = plan->dim * 2 * sizeof(R);
     if (overlaps(state, result, bytes)) return fail(TCP_ERR_INVALID_ARGUMENT, "input and output must not overlap");
-    Workspace ws;
+    tcp::Workspace ws;
     {
         std::lock_guard<std::mutex> lock(plan->ws_mutex);
         for (size_t i = 0; i < plan->ws_free.size(); ++i) {
@@ -941,7 +752,7 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     if (e != cudaSuccess) return cuda_fail(e, "clearing the static scratch status");
     e = cudaMemcpyAsync(dx, state, bytes, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "H2D copy into the static scratch");
-    const DeviceSchedule &ds = plan->sched;
+    const tcp::DeviceSchedule &ds = plan->sched;
     const uint32_t S = kTileBitsC128;
     if (plan->nqubits >= S && ds.host.tile_bits == S) {
         const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();
