@@ -68,6 +68,19 @@ EXPORTED_SYMBOLS = (
     "tcp_mvp_batch_device_status",
 )
 
+# Every symbol include/tcp_solver.h declares.
+SOLVER_SYMBOLS = (
+    "tcp_gram_work_bytes",
+    "tcp_gram",
+    "tcp_block_combine",
+    "tcp_precond_jacobi",
+    "tcp_state_features",
+    "tcp_precond_mlp",
+    "tcp_mlp_inputs",
+    "tcp_mlp_train_work_bytes",
+    "tcp_mlp_train_step",
+)
+
 
 class TcpPlanInfo(ctypes.Structure):
     _fields_ = [
@@ -133,6 +146,21 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mvp_batch_apply.argtypes = [vp, vpp, vpp, vp]
         lib.tcp_mvp_batch_info.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(u32), ctypes.POINTER(u64), ctypes.POINTER(u32)]
         lib.tcp_mvp_batch_device_status.argtypes = [vp]
+        dbl, flt = ctypes.c_double, ctypes.c_float
+        lib.tcp_gram_work_bytes.argtypes = [u32, u32]
+        lib.tcp_gram_work_bytes.restype = ctypes.c_size_t
+        lib.tcp_gram.argtypes = [vp, i32, u32, vp, i32, u32, u64, vp, vp, vp]
+        lib.tcp_block_combine.argtypes = [vp, i32, u32, vp, u32, u64, dbl, dbl, vp, i32, vp]
+        lib.tcp_precond_jacobi.argtypes = [vp, i32, u64, u32, vp, vp, dbl, vp, i32, vp]
+        lib.tcp_state_features.argtypes = [vp, vp, u64, vp]
+        lib.tcp_precond_mlp.argtypes = [vp, i32, u64, u32, vp, vp, vp, dbl, dbl, flt, vp, vp, i32, vp]
+        lib.tcp_mlp_inputs.argtypes = [vp, vp, vp, vp, u32, dbl, dbl, vp, vp, vp]
+        lib.tcp_mlp_train_work_bytes.argtypes = []
+        lib.tcp_mlp_train_work_bytes.restype = ctypes.c_size_t
+        lib.tcp_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp, vp]
+        for name in SOLVER_SYMBOLS:
+            if not name.endswith("_work_bytes"):
+                getattr(lib, name).restype = i32
         for name in EXPORTED_SYMBOLS:
             if name not in ("tcp_last_error",):
                 getattr(lib, name).restype = i32
@@ -265,12 +293,12 @@ class NativeMvpPlan:
 
     def __del__(self) -> None:
         handle = getattr(self, "_handle", None)
-        if handle is not None and handle.value:
-            try:
+        try:
+            if handle is not None and handle.value:
                 self._lib.tcp_mvp_plan_destroy(handle)
-            except Exception:  # interpreter shutdown
-                pass
-            self._handle = ctypes.c_void_p(None)
+                self._handle = None
+        except Exception:  # interpreter shutdown: the library may be gone already
+            pass
 
     # -- metadata ---------------------------------------------------------
     @property

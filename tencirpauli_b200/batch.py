@@ -34,12 +34,12 @@ class BatchedMVP:
 
     def __del__(self) -> None:
         handle = getattr(self, "_handle", None)
-        if handle is not None and handle.value:
-            try:
+        try:
+            if handle is not None and handle.value:
                 self._lib.tcp_mvp_batch_destroy(handle)
-            except Exception:
-                pass
-            self._handle = ctypes.c_void_p(None)
+                self._handle = None
+        except Exception:  # interpreter shutdown
+            pass
 
     @staticmethod
     def _tables(xs: Sequence[Any], ys: Sequence[Any]):

@@ -1,0 +1,230 @@
+"""Block Davidson eigensolver on the B200 MVP.
+
+Finds the ``nev`` lowest eigenpairs of a Hermitian Pauli operator.  The
+reference has no eigensolver of its own: it exposes its MVP plan to SciPy's
+``eigsh`` (``python/tencirpauli/integrations/scipy.py:13-49``); this module is
+the GPU-resident replacement built on ``tcp_mvp_apply_into_device`` and the
+kernels of ``include/tcp_solver.h``.
+
+Precision schedule (both preconditioners use the same one):
+
+1. complex64 basis vectors and the complex64 MVP (FP32 products, Kahan-
+   compensated sums) until every residual is below ``switch_tol`` or stalls;
+2. complex128 basis vectors and the FP64 MVP, restarted from phase 1's Ritz
+   vectors, until every residual is below ``tol``.
+
+Inner products, re-orthogonalisation and the Rayleigh-Ritz projection are
+FP64 in both phases (``tcp_gram`` / ``tcp_block_combine`` accumulate in FP64;
+the small projected eigenproblem is solved with ``torch.linalg.eigh`` in
+FP64).  Every converged pair is judged by the exact FP64-MVP residual
+``||H u - theta u||`` recomputed from the final vector.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Any, List, Optional
+
+import numpy as np
+
+from . import solver_ops
+
+
+@dataclass
+class DavidsonResult:
+    eigenvalues: np.ndarray
+    vectors: Any  # (nev, n) complex128 CUDA tensor
+    residuals: np.ndarray  # exact FP64-MVP residual norms of the returned vectors
+    converged: bool
+    iterations: int
+    mvps: int
+    seconds: float
+    phase_iterations: List[int] = field(default_factory=list)
+    history: List[np.ndarray] = field(default_factory=list)
+    fallbacks: int = 0
+    preconditioner: str = ""
+
+
+class JacobiPreconditioner:
+    """t = -r / (H_ii - theta): the plain diagonal (Davidson) correction."""
+
+    name = "jacobi"
+
+    def prepare(self, plan: Any, diag: Any) -> None:
+        self.diag = diag
+
+    def __call__(self, R: Any, theta: Any, out: Any) -> bool:
+        solver_ops.jacobi(R, self.diag, theta, out)
+        return True
+
+
+def _orthonormalize(T: Any, drop: float) -> Any:
+    """Orthonormal basis of span(T) (rows are vectors) by an eigen-
+    decomposition of the FP64 Gram matrix; directions with relative weight
+    below `drop` are discarded."""
+    import torch
+
+    G = solver_ops.gram(T, T).to("cpu")
+    G = (G + G.conj().T) / 2
+    w, Q = torch.linalg.eigh(G)
+    keep = w > drop * max(float(w.max()), 1e-300)
+    if not bool(keep.any()):
+        return T[:0]
+    S = Q[:, keep] / torch.sqrt(w[keep])
+    out = torch.empty((int(keep.sum()), T.shape[1]), dtype=T.dtype, device=T.device)
+    solver_ops.combine(T, S, out)
+    return out
+
+
+def davidson(
+    plan: Any,
+    nev: int = 4,
+    tol: float = 1e-8,
+    preconditioner: Optional[Any] = None,
+    block: Optional[int] = None,
+    max_subspace: int = 64,
+    keep: Optional[int] = None,
+    switch_tol: float = 1e-4,
+    max_iter: int = 600,
+    seed: int = 0,
+    start: Optional[Any] = None,
+    record_history: bool = False,
+    callback: Optional[Any] = None,
+) -> DavidsonResult:
+    import torch
+
+    from .workloads import random_state_device
+
+    execution = getattr(plan, "_native_plan", plan)
+    n = execution.dimension
+    block = block or nev
+    precond = preconditioner or JacobiPreconditioner()
+    t_start = time.perf_counter()
+    diag = torch.empty(n, dtype=torch.complex128, device="cuda")
+    execution.diagonal_device(diag)
+    precond.prepare(execution, diag)
+    keep = keep or max(nev + block, max_subspace // 2)
+
+    if start is None:
+        X = random_state_device(execution.nqubits, seed=seed, dtype=torch.complex64, nrhs=block)
+    else:
+        X = start
+    iterations = 0
+    mvps = 0
+    fallbacks = 0
+    history: List[np.ndarray] = []
+    phase_iterations: List[int] = []
+    theta = None
+    U = None
+    for dtype, phase_tol in ((torch.complex64, switch_tol), (torch.complex128, tol)):
+        drop = 1e-10 if dtype == torch.complex128 else 1e-5
+        V = torch.empty((max_subspace, n), dtype=dtype, device="cuda")
+        W = torch.empty_like(V)
+        Tm = torch.zeros((max_subspace, max_subspace), dtype=torch.complex128)
+        new = _orthonormalize(X.to(dtype), drop)
+        m = 0
+        phase_it = 0
+        best = np.inf
+        stall = 0
+        while True:
+            k = new.shape[0]
+            if k == 0:
+                break
+            V[m : m + k] = new
+            execution.apply_device(V[m : m + k], W[m : m + k])
+            mvps += k
+            G = solver_ops.gram(V[: m + k], W[m : m + k]).to("cpu")  # (m+k) x k
+            Tm[: m + k, m : m + k] = G
+            Tm[m : m + k, :m] = G[:m].conj().T
+            m += k
+            Th = (Tm[:m, :m] + Tm[:m, :m].conj().T) / 2
+            evals, evecs = torch.linalg.eigh(Th)
+            theta = evals[:nev].clone()
+            S = evecs[:, :nev]
+            U = torch.empty((nev, n), dtype=dtype, device="cuda")
+            HU = torch.empty_like(U)
+            solver_ops.combine(V[:m], S, U)
+            solver_ops.combine(W[:m], S, HU)
+            R = HU.clone()
+            solver_ops.combine(U, -torch.diag(theta.to(torch.complex128)), R, beta=1.0)
+            norms = torch.sqrt(torch.clamp(torch.diagonal(solver_ops.gram(R, R)).real, min=0.0)).cpu().numpy()
+            iterations += 1
+            phase_it += 1
+            if record_history:
+                history.append(norms.copy())
+            if callback is not None:
+                callback(dtype=dtype, iteration=iterations, theta=theta, U=U, R=R, V=V[:m], norms=norms)
+            worst = float(norms.max())
+            if worst < best * 0.9:
+                best, stall = worst, 0
+            else:
+                stall += 1
+            done = bool((norms <= phase_tol).all())
+            stalled = dtype == torch.complex64 and stall >= 15
+            if done or stalled or iterations >= max_iter:
+                if dtype == torch.complex64:
+                    # hand the lowest `keep` Ritz vectors to the FP64 phase
+                    carry = min(keep, m)
+                    X = torch.empty((carry, n), dtype=dtype, device="cuda")
+                    solver_ops.combine(V[:m], evecs[:, :carry], X)
+                break
+            idx = [j for j in range(nev) if norms[j] > phase_tol][:block]
+            Rsel = R[idx].contiguous()
+            Tc = torch.empty_like(Rsel)
+            ok = precond(Rsel, theta[idx], Tc)
+            if not ok or not bool(torch.isfinite(torch.view_as_real(Tc)).all()):
+                fallbacks += 1
+                solver_ops.jacobi(Rsel, diag, theta[idx], Tc)
+            if m + Tc.shape[0] > max_subspace:
+                # thick restart on the lowest `keep` Ritz vectors
+                Sk = evecs[:, :keep]
+                Vn = torch.empty((keep, n), dtype=dtype, device="cuda")
+                Wn = torch.empty_like(Vn)
+                solver_ops.combine(V[:m], Sk, Vn)
+                solver_ops.combine(W[:m], Sk, Wn)
+                V[:keep] = Vn
+                W[:keep] = Wn
+                del Vn, Wn
+                m = keep
+                Tm.zero_()
+                Tm[:m, :m] = torch.diag(evals[:keep].to(torch.complex128))
+            for _ in range(2):  # classical Gram-Schmidt, twice
+                C = solver_ops.gram(V[:m], Tc)
+                solver_ops.combine(V[:m], C, Tc, alpha=-1.0, beta=1.0)
+            new = _orthonormalize(Tc, drop)
+        phase_iterations.append(phase_it)
+        if dtype != torch.complex64:
+            X = U
+        del V, W
+    # exact FP64-MVP residuals of the returned vectors
+    U64 = U.to(torch.complex128)
+    U64 = _orthonormalize(U64, 1e-14) if U64.shape[0] == nev else U64
+    HU64 = torch.empty_like(U64)
+    execution.apply_device(U64, HU64)
+    mvps += U64.shape[0]
+    Gm = solver_ops.gram(U64, HU64).cpu()
+    Gm = (Gm + Gm.conj().T) / 2
+    w, Q = torch.linalg.eigh(Gm)
+    Uf = torch.empty_like(U64)
+    HUf = torch.empty_like(U64)
+    solver_ops.combine(U64, Q, Uf)
+    solver_ops.combine(HU64, Q, HUf)
+    Rf = HUf.clone()
+    solver_ops.combine(Uf, -torch.diag(w.to(torch.complex128)), Rf, beta=1.0)
+    res = torch.sqrt(torch.clamp(torch.diagonal(solver_ops.gram(Rf, Rf)).real, min=0.0)).cpu().numpy()
+    torch.cuda.synchronize()
+    execution.device_status()
+    return DavidsonResult(
+        eigenvalues=w.numpy(),
+        vectors=Uf,
+        residuals=res,
+        converged=bool((res <= tol).all()),
+        iterations=iterations,
+        mvps=mvps,
+        seconds=time.perf_counter() - t_start,
+        phase_iterations=phase_iterations,
+        history=history,
+        fallbacks=fallbacks,
+        preconditioner=getattr(precond, "name", type(precond).__name__),
+    )

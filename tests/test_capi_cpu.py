@@ -16,8 +16,8 @@ from oracle import oracle
 from tencirpauli_b200 import _native
 
 
-def _declared_functions() -> list:
-    header = open(os.path.join(ROOT, "include", "tcp_mvp.h")).read()
+def _declared_functions(name: str = "tcp_mvp.h") -> list:
+    header = open(os.path.join(ROOT, "include", name)).read()
     header = re.sub(r"/\*.*?\*/", "", header, flags=re.S)
     return sorted(set(re.findall(r"\b(tcp_[a-z0-9_]+)\s*\(", header)))
 
@@ -30,6 +30,12 @@ def test_library_loads_and_exports_every_declared_symbol() -> None:
     for name in declared:
         assert hasattr(lib, name), name
     assert lib.tcp_abi_version() == 1
+    solver = _declared_functions("tcp_solver.h")
+    assert set(solver) == set(_native.SOLVER_SYMBOLS)
+    for name in solver:
+        assert hasattr(lib, name), name
+    assert lib.tcp_mlp_train_work_bytes() == 296 * 434 * 4
+    assert lib.tcp_gram_work_bytes(4, 3) == 296 * 12 * 16
 
 
 def test_canonicalize_matches_reference_known_answers() -> None:

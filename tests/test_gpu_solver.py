@@ -1,0 +1,155 @@
+"""GPU tests of the eigensolver kernels, the learned preconditioner's
+training kernels and the Davidson solver, against NumPy restatements
+(``oracle/mlp_oracle.py``) and dense diagonalisation."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU container
+    pytest.skip("CUDA device required", allow_module_level=True)
+
+from tencirpauli_b200 import PauliOperator, precond, solver_ops, workloads  # noqa: E402
+from tencirpauli_b200.davidson import JacobiPreconditioner, davidson  # noqa: E402
+
+
+def _rand(shape, dtype, seed):
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    real = torch.float64 if dtype == torch.complex128 else torch.float32
+    return torch.complex(torch.randn(shape, generator=g, device="cuda", dtype=real), torch.randn(shape, generator=g, device="cuda", dtype=real))
+
+
+def _dense(op: PauliOperator) -> np.ndarray:
+    n = op.nqubits
+    xm, zm, wp = oracle.matrix_terms(n, op.x_words, op.z_words, op.coefficients)
+    dim = 1 << n
+    H = np.zeros((dim, dim), dtype=np.complex128)
+    rows = np.arange(dim, dtype=np.uint64)
+    for x, z, w in zip(xm, zm, wp):
+        cols = rows ^ np.uint64(x)
+        sign = np.where(np.bitwise_count(np.bitwise_and(cols, np.uint64(z))) & 1, -1.0, 1.0)
+        np.add.at(H, (rows.astype(np.int64), cols.astype(np.int64)), w * sign)
+    return H
+
+
+@pytest.mark.parametrize("adt", [torch.complex64, torch.complex128])
+def test_gram_and_combine_match_fp64_numpy(adt) -> None:
+    n = 100003
+    A = _rand((7, n), adt, 1)
+    B = _rand((3, n), torch.complex128, 2)
+    G = solver_ops.gram(A, B).cpu().numpy()
+    An = A.cpu().numpy().astype(np.complex128)
+    Bn = B.cpu().numpy()
+    np.testing.assert_allclose(G, An.conj() @ Bn.T, rtol=1e-12, atol=1e-9)
+    S = torch.complex(torch.randn(7, 3, dtype=torch.float64), torch.randn(7, 3, dtype=torch.float64))
+    out = _rand((3, n), torch.complex128, 3)
+    before = out.cpu().numpy()
+    solver_ops.combine(A, S, out, alpha=0.5, beta=-2.0)
+    expect = 0.5 * (S.numpy().T @ An) - 2.0 * before
+    np.testing.assert_allclose(out.cpu().numpy(), expect, rtol=1e-12, atol=1e-10)
+
+
+def test_features_inputs_and_corrections_match_oracle() -> None:
+    op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(3, 4, 1.0, 0.4))
+    plan = op.native_mvp_plan()
+    feats = solver_ops.state_features(plan).cpu().numpy()
+    xm, zm, wp = oracle.matrix_terms(op.nqubits, op.x_words, op.z_words, op.coefficients)
+    ref = mo.state_features(op.nqubits, xm, zm, wp)
+    np.testing.assert_allclose(feats[:, :7], ref[:, :7], rtol=1e-6, atol=1e-5)
+    scale = precond.energy_scale(op)
+    params = np.random.default_rng(4).normal(scale=0.4, size=mo.NPARAM).astype(np.float32)
+    R = _rand((2, plan.dimension), torch.complex128, 5)
+    theta = torch.tensor([-6.0137, -5.4921], dtype=torch.float64)
+    out = torch.empty_like(R)
+    dg = torch.empty(plan.dimension, dtype=torch.complex128, device="cuda")
+    plan._native_plan.diagonal_device(dg)
+    solver_ops.mlp_precondition(R, torch.from_numpy(feats).cuda(), dg, theta, torch.from_numpy(params).cuda(), scale, out)
+    for j in range(2):
+        expect = mo.mlp_correction(params, feats.astype(np.float64), R[j].cpu().numpy(), float(theta[j]), scale)
+        np.testing.assert_allclose(out[j].cpu().numpy(), expect, rtol=2e-4, atol=1e-6 * np.abs(expect).max())
+    diag = torch.empty(plan.dimension, dtype=torch.complex128, device="cuda")
+    plan._native_plan.diagonal_device(diag)
+    jac = torch.empty_like(R)
+    solver_ops.jacobi(R, diag, theta, jac)
+    np.testing.assert_allclose(jac[1].cpu().numpy(), mo.jacobi(diag.cpu().numpy(), R[1].cpu().numpy(), -5.4921), rtol=1e-12)
+    # network inputs for sampled rows
+    rows = torch.tensor([0, 5, 17, 4095], dtype=torch.int64, device="cuda")
+    which = torch.tensor([0, 1, 1, 0], dtype=torch.int32, device="cuda")
+    X, den = solver_ops.mlp_inputs(torch.from_numpy(feats).cuda(), rows, theta, which, scale)
+    for s, (r, w) in enumerate(zip(rows.cpu().numpy(), which.cpu().numpy())):
+        xr, dr = mo.inputs(feats[r : r + 1].astype(np.float64), float(theta[w]), scale)
+        np.testing.assert_allclose(X[s].cpu().numpy(), xr[0], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(den[s].item(), dr[0], rtol=1e-6)
+
+
+def test_training_gradient_matches_oracle_and_adam_reduces_loss() -> None:
+    rng = np.random.default_rng(0)
+    count = 3000
+    X = rng.normal(size=(count, mo.IN)).astype(np.float32)
+    den = (rng.uniform(0.5, 3.0, size=count) * rng.choice([-1, 1], size=count)).astype(np.float32)
+    r = rng.normal(size=count) + 1j * rng.normal(size=count)
+    e = 0.8 * (-r / den) + 0.1 * (rng.normal(size=count) + 1j * rng.normal(size=count))
+    a = (np.abs(r) ** 2).astype(np.float32)
+    b = (np.conj(e) * r).real.astype(np.float32)
+    e2 = (np.abs(e) ** 2).astype(np.float32)
+    wt = np.full(count, 1.0 / e2.sum(), dtype=np.float32)
+    p = rng.normal(scale=0.3, size=mo.NPARAM).astype(np.float32)
+    dev = [torch.from_numpy(v).cuda() for v in (X, den, a, b, e2, wt)]
+    params = torch.from_numpy(p.copy()).cuda()
+    trainer = solver_ops.MLPTrainer(params)
+    trainer.step(*dev, lr=0.0)  # gradient only
+    loss_ref, grad_ref = mo.loss_and_grad(p.astype(np.float64), X.astype(np.float64), den.astype(np.float64), a, b, e2, wt)
+    assert abs(trainer.loss.item() - loss_ref) <= 1e-4 * abs(loss_ref)
+    g = trainer.grad.cpu().numpy()
+    np.testing.assert_allclose(g, grad_ref, rtol=2e-3, atol=2e-5 * np.abs(grad_ref).max())
+    np.testing.assert_array_equal(params.cpu().numpy(), p)  # lr = 0 leaves the weights alone
+    first = trainer.loss.item()
+    for _ in range(200):
+        trainer.step(*dev, lr=1e-2)
+    assert trainer.loss.item() < 0.5 * first
+
+
+def test_davidson_matches_dense_eigenvalues_with_exact_residuals() -> None:
+    op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(3, 4, 1.0, 0.5))
+    plan = op.native_mvp_plan()
+    H = _dense(op)
+    ref = np.linalg.eigvalsh(H)[:4]
+    res = davidson(plan, nev=4, tol=1e-8, seed=3)
+    assert res.converged, res.residuals
+    np.testing.assert_allclose(res.eigenvalues, ref, rtol=0, atol=1e-9)
+    assert (res.residuals <= 1e-8).all()
+    # the returned vectors satisfy H u = theta u to the tolerance (dense check)
+    U = res.vectors.cpu().numpy()
+    for j in range(4):
+        assert np.linalg.norm(H @ U[j] - res.eigenvalues[j] * U[j]) <= 1e-8
+    assert res.phase_iterations and len(res.phase_iterations) == 2
+
+
+def test_learned_preconditioner_runs_and_untrained_equals_jacobi() -> None:
+    op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(4, 4, 1.0, 0.3))
+    plan = op.native_mvp_plan()
+    untrained = precond.MLPPreconditioner(precond.init_params(0), scale=precond.energy_scale(op))
+    jacobi = JacobiPreconditioner()
+    diag = torch.empty(plan.dimension, dtype=torch.complex128, device="cuda")
+    plan._native_plan.diagonal_device(diag)
+    untrained.prepare(plan._native_plan, diag)
+    jacobi.prepare(plan._native_plan, diag)
+    R = _rand((3, plan.dimension), torch.complex128, 9)
+    theta = torch.tensor([-9.0, -8.5, -8.0], dtype=torch.float64)
+    t_mlp, t_jac = torch.empty_like(R), torch.empty_like(R)
+    untrained(R, theta, t_mlp)
+    jacobi(R, theta, t_jac)
+    rel = torch.linalg.vector_norm(t_mlp - t_jac) / torch.linalg.vector_norm(t_jac)
+    assert float(rel) == 0.0  # c = 0 is the Jacobi correction, bit for bit
+    res = davidson(plan, nev=4, tol=1e-8, seed=1, preconditioner=untrained)
+    ref = davidson(plan, nev=4, tol=1e-8, seed=1)
+    assert res.converged and ref.converged
+    np.testing.assert_allclose(res.eigenvalues, ref.eigenvalues, atol=1e-9)
