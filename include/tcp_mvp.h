@@ -211,6 +211,12 @@ int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const double *stat
                                     uint64_t state_len, double *result, uint64_t result_len,
                                     void *stream);
 
+/* Self-test of the bounded device waits (no counterpart in the reference): a
+ * kernel waits, with a limit of `limit_ns` (at most 100 ms), on an mbarrier
+ * that nothing completes, and reports the expiry through the plan's status
+ * word.  Returns TCP_ERR_DEVICE_TIMEOUT when the wait gave up as designed. */
+int tcp_selftest_bounded_wait(const tcp_mvp_plan *plan, uint64_t limit_ns);
+
 /* Synchronise the plan's device and report (then clear) any device-side error
  * flag raised by kernels of this plan. */
 int tcp_mvp_plan_device_status(const tcp_mvp_plan *plan);

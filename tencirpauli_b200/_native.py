@@ -57,6 +57,7 @@ EXPORTED_SYMBOLS = (
     "tcp_mvp_apply_into_device",
     "tcp_mvp_apply_into_host_noalloc",
     "tcp_mvp_plan_device_status",
+    "tcp_selftest_bounded_wait",
     "tcp_mvp_transition_count",
     "tcp_mvp_diagonal_device",
     "tcp_mvp_batch_create",
@@ -136,6 +137,7 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mvp_apply_into_device.argtypes = [vp, vp, vp, u64, u32, i32, vp]
         lib.tcp_mvp_apply_into_host_noalloc.argtypes = [vp, f64p, u64, f64p, u64, vp]
         lib.tcp_mvp_plan_device_status.argtypes = [vp]
+        lib.tcp_selftest_bounded_wait.argtypes = [vp, u64]
         lib.tcp_mvp_transition_count.argtypes = [vp, u64p]
         lib.tcp_mvp_diagonal_device.argtypes = [vp, vp, u64, vp]
         vpp = ctypes.POINTER(vp)

@@ -79,13 +79,14 @@ __device__ __forceinline__ unsigned long long global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait on an mbarrier phase: returns false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: returns false after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long start = global_ns();
     for (uint32_t spin = 1;; ++spin) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((spin & 255u) == 0u && global_ns() - start > kWaitLimitNs) return false;
+        if ((spin & 255u) == 0u && global_ns() - start > limit_ns) return false;
     }
 }
 

@@ -683,6 +683,39 @@ extern "C" int tcp_mvp_diagonal_device(const tcp_mvp_plan *plan, void *d_diag, u
 }
 
 // ---------------------------------------------------------------------------
+// Self-test of the bounded device waits: one CTA arms an mbarrier for bytes
+// that no copy will ever deliver and waits on it with a short limit; the wait
+// gives up, the kernel records a timeout in the plan's status word and exits.
+// No copy is in flight, so nothing touches the abandoned barrier afterwards.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_wait_selftest(unsigned long long limit_ns, int *err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16);  // 16 bytes that never arrive
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, limit_ns);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+    }
+}
+}  // namespace
+
+extern "C" int tcp_selftest_bounded_wait(const tcp_mvp_plan *plan, uint64_t limit_ns) {
+    int st = check_plan(plan);
+    if (st) return st;
+    if (limit_ns > 100000000ull) return fail(TCP_ERR_INVALID_ARGUMENT, "self-test wait limit above 100 ms");
+    k_wait_selftest<<<1, 32>>>(limit_ns, plan->d_err);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "self-test kernel launch");
+    return tcp_mvp_plan_device_status(plan);
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free host apply (tcp_mvp_apply_into_host_noalloc).
 //
 // For callers that may not allocate device memory while applying.  The state
