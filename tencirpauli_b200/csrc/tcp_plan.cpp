@@ -292,15 +292,37 @@ extern "C" int tcp_pauli_canonicalize(uint32_t nqubits, uint64_t count, const ui
     };
     std::vector<uint64_t> idx(count);
     std::iota(idx.begin(), idx.end(), 0);
-    std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
-        int r = word_less(a, b);
-        if (r) return r < 0;
+    auto tie_break = [&](uint64_t a, uint64_t b) {
         uint64_t ar = bits_of(coefficients[2 * a]), br = bits_of(coefficients[2 * b]);
         if (ar != br) return ar < br;
         uint64_t ai = bits_of(coefficients[2 * a + 1]), bi = bits_of(coefficients[2 * b + 1]);
         if (ai != bi) return ai < bi;
         return a < b;
-    });
+    };
+    if (nqubits <= 64) {
+        // Word order (word.rs:240-254) as a 128-bit integer key: the 2-bit code
+        // of qubit 0 is the most significant digit.
+        std::vector<std::pair<uint64_t, uint64_t>> key(count);
+        for (uint64_t t = 0; t < count; ++t) {
+            uint64_t hi = 0, lo = 0;
+            for (uint32_t q = 0; q < nqubits; ++q) {
+                const uint64_t c = codes[t * nqubits + q];
+                const uint32_t pos = 2 * (63 - q);  // digit position inside 128 bits
+                if (pos >= 64) hi |= c << (pos - 64); else lo |= c << pos;
+            }
+            key[t] = {hi, lo};
+        }
+        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            if (key[a] != key[b]) return key[a] < key[b];
+            return tie_break(a, b);
+        });
+    } else {
+        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            int r = word_less(a, b);
+            if (r) return r < 0;
+            return tie_break(a, b);
+        });
+    }
     uint64_t out = 0;
     for (uint64_t i = 0; i < count;) {
         uint64_t j = i;

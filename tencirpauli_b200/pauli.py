@@ -250,6 +250,13 @@ class PauliOperator:
             return BackendMVPPlan.from_operator(self, max_bytes=max_bytes)
         raise ValueError("target must be one of 'native_mvp' or 'backend_mvp'")
 
+    def backend_mvp_plan(self, *, max_bytes: Optional[int] = DEFAULT_MAX_BYTES) -> Any:
+        """Versioned pure-array plan (``pauli.py:953-983`` of the reference)
+        whose executor runs on the device."""
+        from .backend import BackendMVPPlan
+
+        return BackendMVPPlan.from_operator(self, max_bytes=max_bytes)
+
     def to_scipy_linear_operator(self, *, max_bytes: Optional[int] = DEFAULT_MAX_BYTES) -> Any:
         from .integrations.scipy import to_scipy_linear_operator
 
