@@ -80,6 +80,15 @@ int tcp_mlp_train_step(const float *d_X, const float *d_den, const float *d_a, c
                        float *d_v, float *d_work, float lr, uint32_t step, float *d_grad_out,
                        float *d_loss_out, void *stream);
 
+/* Network output c for `count` input rows (count x TCP_MLP_IN floats). */
+int tcp_mlp_forward(const float *d_X, uint32_t count, const float *d_params, float *d_out, void *stream);
+
+/* Gradient of any loss from its derivatives dL/dc (d_dc, one per sample):
+ * back-propagates through the network, writes the summed gradient to
+ * d_grad_out (if non-null) and, with lr > 0, applies one Adam step. */
+int tcp_mlp_backward_step(const float *d_X, const float *d_dc, uint32_t count, float *d_params, float *d_m,
+                          float *d_v, float *d_work, float lr, uint32_t step, float *d_grad_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

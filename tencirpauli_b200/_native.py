@@ -80,6 +80,8 @@ SOLVER_SYMBOLS = (
     "tcp_mlp_inputs",
     "tcp_mlp_train_work_bytes",
     "tcp_mlp_train_step",
+    "tcp_mlp_forward",
+    "tcp_mlp_backward_step",
 )
 
 
@@ -160,6 +162,8 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mlp_train_work_bytes.argtypes = []
         lib.tcp_mlp_train_work_bytes.restype = ctypes.c_size_t
         lib.tcp_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp, vp]
+        lib.tcp_mlp_forward.argtypes = [vp, u32, vp, vp, vp]
+        lib.tcp_mlp_backward_step.argtypes = [vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp]
         for name in SOLVER_SYMBOLS:
             if not name.endswith("_work_bytes"):
                 getattr(lib, name).restype = i32

@@ -300,8 +300,8 @@ constexpr int kTrainStride = IN + 4 * HID + 1;  // x, h1, h2, dh1, dh2, dc
 __global__ void __launch_bounds__(kTrainChunk)
     k_mlp_train(const float *__restrict__ X, const float *__restrict__ den, const float *__restrict__ a,
                 const float *__restrict__ b, const float *__restrict__ e2, const float *__restrict__ wt,
-                uint32_t count, const float *__restrict__ wglob, float *__restrict__ grad_partial,
-                float *__restrict__ loss_partial) {
+                const float *__restrict__ dc_in, uint32_t count, const float *__restrict__ wglob,
+                float *__restrict__ grad_partial, float *__restrict__ loss_partial) {
     __shared__ float w[NPARAM];
     __shared__ float act[kTrainChunk][kTrainStride];
     __shared__ float lsum[kTrainChunk];
@@ -321,10 +321,15 @@ __global__ void __launch_bounds__(kTrainChunk)
 #pragma unroll
             for (int i = 0; i < IN; ++i) x[i] = X[static_cast<size_t>(sidx) * IN + i];
             const float c = mlp_forward(w, x, h1, h2);
-            const float g = -expf(c) / den[sidx];
-            const float as = a[sidx], bs = b[sidx], ws = wt[sidx];
-            loss += ws * (g * g * as - 2.f * g * bs + e2[sidx]);
-            const float dc = ws * (2.f * g * as - 2.f * bs) * g;  // dL/dc
+            float dc;
+            if (dc_in != nullptr) {  // caller-supplied dL/dc (any loss on the outputs)
+                dc = dc_in[sidx];
+            } else {
+                const float g = -expf(c) / den[sidx];
+                const float as = a[sidx], bs = b[sidx], ws = wt[sidx];
+                loss += ws * (g * g * as - 2.f * g * bs + e2[sidx]);
+                dc = ws * (2.f * g * as - 2.f * bs) * g;  // dL/dc
+            }
             float dh2[HID];
 #pragma unroll
             for (int i = 0; i < HID; ++i) dh2[i] = dc * w[OFF_W3 + i] * (1.f - h2[i] * h2[i]);
@@ -392,6 +397,20 @@ __global__ void k_sum_losses(const float *__restrict__ partial, uint32_t blocks,
         float l = 0.f;
         for (uint32_t b = 0; b < blocks; ++b) l += partial[b];
         *out = l;
+    }
+}
+
+// Network output c for every sample.
+__global__ void k_mlp_forward(const float *__restrict__ X, uint32_t count, const float *__restrict__ wglob,
+                              float *__restrict__ out) {
+    __shared__ float w[NPARAM];
+    for (int e = threadIdx.x; e < NPARAM; e += blockDim.x) w[e] = wglob[e];
+    __syncthreads();
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
+        float x[IN], h1[HID], h2[HID];
+#pragma unroll
+        for (int i = 0; i < IN; ++i) x[i] = X[static_cast<size_t>(s) * IN + i];
+        out[s] = mlp_forward(w, x, h1, h2);
     }
 }
 
@@ -536,6 +555,30 @@ extern "C" int tcp_mlp_inputs(const float *d_features, const uint64_t *d_rows, c
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "mlp input kernel launch");
 }
 
+extern "C" int tcp_mlp_forward(const float *d_X, uint32_t count, const float *d_params, float *d_out, void *stream) {
+    if (!d_X || !d_params || !d_out) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    if (count == 0) return TCP_OK;
+    k_mlp_forward<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_X, count, d_params, d_out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "mlp forward launch");
+}
+
+extern "C" int tcp_mlp_backward_step(const float *d_X, const float *d_dc, uint32_t count, float *d_params, float *d_m,
+                                     float *d_v, float *d_work, float lr, uint32_t step, float *d_grad_out,
+                                     void *stream) {
+    if (!d_X || !d_dc || !d_params || !d_work) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    if (lr != 0.f && (!d_m || !d_v || step == 0)) return fail(TCP_ERR_INVALID_ARGUMENT, "Adam state missing");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float *grad_partial = d_work;
+    float *loss_partial = d_work + static_cast<size_t>(TCP_MLP_TRAIN_BLOCKS) * TCP_MLP_PARAMS;
+    k_mlp_train<<<TCP_MLP_TRAIN_BLOCKS, kTrainChunk, 0, s>>>(d_X, nullptr, nullptr, nullptr, nullptr, nullptr, d_dc,
+                                                             count, d_params, grad_partial, loss_partial);
+    k_adam<<<(TCP_MLP_PARAMS + 255) / 256, 256, 0, s>>>(d_params, d_m, d_v, grad_partial, TCP_MLP_TRAIN_BLOCKS, 1.f, lr,
+                                                       0.9f, 0.999f, 1e-8f, step, d_grad_out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "mlp backward launch");
+}
+
 extern "C" size_t tcp_mlp_train_work_bytes(void) {
     return static_cast<size_t>(TCP_MLP_TRAIN_BLOCKS) * (TCP_MLP_PARAMS + 1) * sizeof(float);
 }
@@ -551,8 +594,8 @@ extern "C" int tcp_mlp_train_step(const float *d_X, const float *d_den, const fl
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     float *grad_partial = d_work;
     float *loss_partial = d_work + static_cast<size_t>(TCP_MLP_TRAIN_BLOCKS) * TCP_MLP_PARAMS;
-    k_mlp_train<<<TCP_MLP_TRAIN_BLOCKS, kTrainChunk, 0, s>>>(d_X, d_den, d_a, d_b, d_e2, d_wt, count, d_params,
-                                                             grad_partial, loss_partial);
+    k_mlp_train<<<TCP_MLP_TRAIN_BLOCKS, kTrainChunk, 0, s>>>(d_X, d_den, d_a, d_b, d_e2, d_wt, nullptr, count,
+                                                             d_params, grad_partial, loss_partial);
     k_adam<<<(TCP_MLP_PARAMS + 255) / 256, 256, 0, s>>>(d_params, d_m, d_v, grad_partial, TCP_MLP_TRAIN_BLOCKS, 1.f, lr,
                                                        0.9f, 0.999f, 1e-8f, step, d_grad_out);
     if (d_loss_out) k_sum_losses<<<1, 32, 0, s>>>(loss_partial, TCP_MLP_TRAIN_BLOCKS, d_loss_out);

@@ -234,3 +234,167 @@ def train_from_lattices(
     data = _cat(sets)
     params, losses = train(data, steps=steps, seed=seed)
     return params, {"samples": data.size, "losses": losses, "lattices": list(lattices), "steps": steps}
+
+
+# ---------------------------------------------------------------------------
+# Alignment objective: train the network so that its correction points along
+# the direction Davidson is missing.  For a Ritz vector u of a trajectory with
+# basis V and residual r, the ideal new direction is e = (I - V V^H) v, with v
+# the projection of u onto the exact eigenspace.  The correction t = g o r
+# (g = -exp(c) / den per basis state) is scored by the squared cosine between
+# t, made orthogonal to u, and e:
+#     L = 1 - |<e, t>|^2 / (||e||^2 (||t||^2 - |<u, t>|^2))
+# (<e, t> needs no projection since e is orthogonal to V).  The loss is
+# invariant to the scale of t, as the Davidson expansion is.
+# ---------------------------------------------------------------------------
+@dataclass
+class AlignmentSets:
+    X: Any  # (N, TCP_MLP_IN) float32 network inputs, all basis states of every set
+    den: Any  # (N,) float32
+    alpha: Any  # (N,) complex128: conj(e_i) r_i
+    a: Any  # (N,) float64: |r_i|^2
+    gamma: Any  # (N,) complex128: conj(u_i) r_i
+    E: Any  # (S,) float64: ||e||^2 per set
+    seg: Any  # (N,) int64 set index
+    nsets: int
+
+
+def _cat_alignment(parts: Sequence[AlignmentSets]) -> AlignmentSets:
+    import torch
+
+    offset = 0
+    segs = []
+    for p in parts:
+        segs.append(p.seg + offset)
+        offset += p.nsets
+    return AlignmentSets(
+        X=torch.cat([p.X for p in parts]),
+        den=torch.cat([p.den for p in parts]),
+        alpha=torch.cat([p.alpha for p in parts]),
+        a=torch.cat([p.a for p in parts]),
+        gamma=torch.cat([p.gamma for p in parts]),
+        E=torch.cat([p.E for p in parts]),
+        seg=torch.cat(segs),
+        nsets=offset,
+    )
+
+
+def collect_alignment_sets(
+    op: Any, nev: int = 4, every: int = 3, max_iterations: int = 45, seed: int = 0, tol_exact: float = 1e-10
+) -> Optional[AlignmentSets]:
+    """Full-vector training sets from a Jacobi Davidson trajectory on `op`."""
+    import torch
+
+    from .davidson import davidson
+
+    plan = op.native_mvp_plan()
+    exact = davidson(plan, nev=nev + 2, tol=tol_exact, seed=seed + 1000)
+    lam = torch.from_numpy(exact.eigenvalues)
+    Uex = exact.vectors
+    scale = energy_scale(op)
+    features = solver_ops.state_features(plan)
+    n = plan.dimension
+    all_rows = torch.arange(n, dtype=torch.int64, device="cuda")
+    zeros = torch.zeros(n, dtype=torch.int32, device="cuda")
+    parts: List[AlignmentSets] = []
+
+    def record(dtype, iteration, theta, U, R, V, norms):
+        if iteration > max_iterations or iteration % every:
+            return
+        for j in range(U.shape[0]):
+            if not (1e-9 < norms[j] < 1e-1):
+                continue
+            dist = torch.abs(lam - float(theta[j]))
+            near = dist < 1e-6 + 1e-3 * float(norms[j])
+            if not bool(near.any()):
+                near = dist == dist.min()
+            Q = Uex[near.nonzero().flatten().cuda()]
+            uj = U[j : j + 1].to(torch.complex128).contiguous()
+            c = solver_ops.gram(Q, uj)  # Q^H u
+            v = torch.empty_like(uj)
+            solver_ops.combine(Q, c, v)
+            e = v.clone()
+            for _ in range(2):  # e = (I - V V^H) v
+                C = solver_ops.gram(V, e)
+                solver_ops.combine(V, C, e, alpha=-1.0, beta=1.0)
+            E = float(torch.linalg.vector_norm(e) ** 2)
+            if E <= 1e-30:
+                continue
+            X, den = solver_ops.mlp_inputs(features, all_rows, theta[j : j + 1], zeros, scale)
+            r = R[j].to(torch.complex128)
+            u = uj[0]
+            parts.append(
+                AlignmentSets(
+                    X=X,
+                    den=den,
+                    alpha=torch.conj(e[0]) * r,
+                    a=(r.real**2 + r.imag**2),
+                    gamma=torch.conj(u) * r,
+                    E=torch.tensor([E], dtype=torch.float64, device="cuda"),
+                    seg=torch.zeros(n, dtype=torch.int64, device="cuda"),
+                    nsets=1,
+                )
+            )
+
+    davidson(plan, nev=nev, tol=1e-9, seed=seed, callback=record, max_iter=max_iterations + 1)
+    return _cat_alignment(parts) if parts else None
+
+
+def alignment_loss_and_dc(c: Any, data: AlignmentSets, clamp: float = 4.0):
+    """Mean alignment loss over the sets and dL/dc per basis state."""
+    import torch
+
+    S = data.nsets
+    cc = torch.clamp(c.double(), -clamp, clamp)
+    g = -torch.exp(cc) / data.den.double()
+    A = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add_(0, data.seg, g * data.alpha)
+    B = torch.zeros(S, dtype=torch.float64, device="cuda").index_add_(0, data.seg, g * g * data.a)
+    C = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add_(0, data.seg, g * data.gamma)
+    D = torch.clamp(B - C.abs() ** 2, min=1e-300)
+    A2 = A.abs() ** 2
+    loss = torch.mean(1.0 - A2 / (data.E * D))
+    As, Cs, Ds, Es, A2s = A[data.seg], C[data.seg], D[data.seg], data.E[data.seg], A2[data.seg]
+    dA2 = 2.0 * (torch.conj(As) * data.alpha).real
+    dD = 2.0 * g * data.a - 2.0 * (torch.conj(Cs) * data.gamma).real
+    dLdg = -(dA2 * Ds - A2s * dD) / (Es * Ds * Ds) / S
+    inside = (c.double() > -clamp) & (c.double() < clamp)
+    dc = torch.where(inside, dLdg * g, torch.zeros_like(g))
+    return float(loss), dc.float()
+
+
+def train_alignment(
+    data: AlignmentSets, params: Optional[np.ndarray] = None, steps: int = 300, lr: float = 3e-3, seed: int = 0, log_every: int = 50
+) -> Tuple[np.ndarray, List[float]]:
+    """Adam on the alignment loss: forward and backward through the device
+    kernels (tcp_mlp_forward, tcp_mlp_backward_step); the loss-level
+    derivative dL/dc is elementwise GPU arithmetic."""
+    import torch
+
+    p = torch.from_numpy(init_params(seed) if params is None else np.asarray(params, np.float32)).cuda()
+    trainer = solver_ops.MLPTrainer(p)
+    losses: List[float] = []
+    for s in range(steps):
+        c = solver_ops.mlp_forward(data.X, p)
+        loss, dc = alignment_loss_and_dc(c, data)
+        trainer.backward_step(data.X, dc, lr)
+        if s % log_every == 0 or s == steps - 1:
+            losses.append(loss)
+    return p.cpu().numpy(), losses
+
+
+def train_alignment_from_lattices(
+    lattices: Iterable[Tuple[int, int, float]], steps: int = 300, seed: int = 0, every: int = 3
+) -> Tuple[np.ndarray, Dict[str, Any]]:
+    from .pauli import PauliOperator
+    from .workloads import j1j2_periodic
+
+    parts = []
+    for i, (lx, ly, j2) in enumerate(lattices):
+        op = PauliOperator.from_code_arrays(*j1j2_periodic(lx, ly, 1.0, j2))
+        s = collect_alignment_sets(op, seed=seed + i, every=every)
+        if s is not None:
+            parts.append(s)
+    data = _cat_alignment(parts)
+    params, losses = train_alignment(data, steps=steps, seed=seed)
+    return params, {"objective": "alignment", "sets": data.nsets, "states": int(data.X.shape[0]), "losses": losses,
+                    "lattices": list(lattices), "steps": steps}

@@ -171,6 +171,16 @@ def mlp_inputs(features: Any, rows: Any, theta: Any, which: Any, scale: float, e
     return X, den
 
 
+def mlp_forward(X: Any, params: Any, out: Any = None, stream: Any = None) -> Any:
+    import torch
+
+    count = int(X.shape[0])
+    if out is None:
+        out = torch.empty(count, dtype=torch.float32, device="cuda")
+    _native.raise_for_status(_lib().tcp_mlp_forward(_ptr(X), count, _ptr(params), _ptr(out), _stream(stream)))
+    return out
+
+
 class MLPTrainer:
     """Device training state (parameters, Adam moments, scratch)."""
 
@@ -184,6 +194,17 @@ class MLPTrainer:
         self.grad = torch.empty_like(params)
         self.loss = torch.empty(1, dtype=torch.float32, device="cuda")
         self.step_count = 0
+
+    def backward_step(self, X, dc, lr: float, stream: Any = None) -> None:
+        """Weight gradient from given dL/dc per sample; Adam step when lr > 0."""
+        if lr > 0:
+            self.step_count += 1
+        _native.raise_for_status(
+            _lib().tcp_mlp_backward_step(
+                _ptr(X), _ptr(dc), int(X.shape[0]), _ptr(self.params), _ptr(self.m), _ptr(self.v), _ptr(self.work), lr,
+                max(self.step_count, 1), _ptr(self.grad), _stream(stream),
+            )
+        )
 
     def step(self, X, den, a, b, e2, wt, lr: float, stream: Any = None) -> None:
         if lr > 0:

@@ -153,3 +153,37 @@ def test_learned_preconditioner_runs_and_untrained_equals_jacobi() -> None:
     ref = davidson(plan, nev=4, tol=1e-8, seed=1)
     assert res.converged and ref.converged
     np.testing.assert_allclose(res.eigenvalues, ref.eigenvalues, atol=1e-9)
+
+
+def test_alignment_gradient_matches_autograd_and_forward_matches_oracle() -> None:
+    from tencirpauli_b200.precond import AlignmentSets, alignment_loss_and_dc
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    n, S = 4000, 3
+    seg = torch.arange(n, device="cuda") % S
+    c = 0.3 * torch.randn(n, device="cuda", dtype=torch.float64, generator=g)
+    den = (torch.rand(n, device="cuda", generator=g, dtype=torch.float64) + 0.5).float()
+    r = _rand((n,), torch.complex128, 11)
+    e = _rand((n,), torch.complex128, 12)
+    u = _rand((n,), torch.complex128, 13)
+    unorm = torch.zeros(S, dtype=torch.float64, device="cuda").index_add_(0, seg, u.abs() ** 2).sqrt()
+    u = u / unorm[seg]  # a unit vector per set, as Ritz vectors are
+    E = torch.zeros(S, dtype=torch.float64, device="cuda").index_add_(0, seg, (e.abs() ** 2))
+    data = AlignmentSets(X=None, den=den, alpha=torch.conj(e) * r, a=r.abs() ** 2, gamma=torch.conj(u) * r, E=E, seg=seg, nsets=S)
+    loss, dc = alignment_loss_and_dc(c.float(), data)
+    cv = c.float().double().clone().requires_grad_(True)
+    gg = -torch.exp(cv) / den.double()
+    A = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add(0, seg, gg * data.alpha)
+    B = torch.zeros(S, dtype=torch.float64, device="cuda").index_add(0, seg, gg * gg * data.a)
+    C = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add(0, seg, gg * data.gamma)
+    ref = torch.mean(1 - A.abs() ** 2 / (E * (B - C.abs() ** 2)))
+    ref.backward()
+    assert abs(loss - float(ref.detach())) <= 1e-10
+    np.testing.assert_allclose(dc.cpu().numpy(), cv.grad.cpu().numpy(), rtol=1e-4, atol=1e-9)
+    # device forward pass against the NumPy restatement
+    params = np.random.default_rng(5).normal(scale=0.4, size=mo.NPARAM).astype(np.float32)
+    X = np.random.default_rng(6).normal(size=(257, mo.IN)).astype(np.float32)
+    out = solver_ops.mlp_forward(torch.from_numpy(X).cuda(), torch.from_numpy(params).cuda()).cpu().numpy()
+    ref_c, _ = mo.forward(params.astype(np.float64), X.astype(np.float64))
+    np.testing.assert_allclose(out, ref_c, rtol=1e-4, atol=1e-5)
