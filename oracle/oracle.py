@@ -16,6 +16,13 @@ project ``crates/tencir-pauli-core/src``):
 * :func:`apply_xmask_diagonal` -- ``hamiltonian.rs:79-147,233-235`` (eager plan)
 * :func:`transition_count`   -- ``hamiltonian.rs:166-179``
 * :func:`apply_rows`         -- the TermDirect row loop on selected rows only
+
+U(1) sector items (``oracle/u1_oracle.c``, paths in ``sector.rs``):
+
+* :func:`u1_dimension` / :func:`u1_rank` / :func:`u1_unrank` -- ``:79-238,310-341``
+* :func:`u1_apply`           -- ``U1LazyMvpPlan::apply_into`` (``:579-643``)
+* :func:`u1_csr`             -- ``U1RestrictedOperator::new`` / ``csr`` (``:345-431``)
+* :func:`number_commutator`  -- ``operator.rs:396-444`` with levels (0, 1)
 """
 
 from __future__ import annotations
@@ -61,6 +68,15 @@ def _load() -> ctypes.CDLL:
         lib.oracle_packed_word_count.argtypes = [u32]
         lib.oracle_packed_word_count.restype = u32
         lib.oracle_max_threads.restype = i32
+        lib.oracle_u1_dimension.argtypes = [u32, u32, _u64p]
+        lib.oracle_u1_rank.argtypes = [u32, u32, _u64p, _u64p]
+        lib.oracle_u1_unrank.argtypes = [u32, u32, u64, _u64p]
+        lib.oracle_u1_apply.argtypes = [u32, u32, u64, _u64p, _u64p, _f64p, _f64p, _f64p, _u64p, _u64p]
+        lib.oracle_u1_csr.argtypes = [u32, u32, u64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p, u64, _u64p, _u64p, _u64p]
+        lib.oracle_number_commutator.argtypes = [u32, u64, _u64p, _u64p, _f64p, _u64p]
+        for name in ("oracle_u1_dimension", "oracle_u1_rank", "oracle_u1_unrank", "oracle_u1_apply",
+                     "oracle_u1_csr", "oracle_number_commutator"):
+            getattr(lib, name).restype = i32
         for name in (
             "oracle_encode_codes",
             "oracle_canonicalize",
@@ -280,3 +296,117 @@ def mvp(nqubits: int, codes: np.ndarray, coefficients: np.ndarray, state: np.nda
     xw, zw, c = canonicalize(nqubits, codes, coefficients)
     xm, zm, wp = matrix_terms(nqubits, xw, zw, c)
     return apply_term_direct(nqubits, xm, zm, wp, state, threads)
+
+
+# --------------------------- U(1) sector oracle ------------------------------
+class OracleLeakage(OracleError):
+    """``PauliError::SectorLeakage``: the lowest leaking source and its weight."""
+
+    def __init__(self, source: int, weight: int) -> None:
+        super().__init__(11, f"leakage from source {source} to weight {weight}")
+        self.source = source
+        self.weight = weight
+
+
+def u1_dimension(nqubits: int, particle_number: int) -> int:
+    out = np.zeros(1, np.uint64)
+    status = _load().oracle_u1_dimension(nqubits, particle_number, _p(out, _u64p))
+    if status:
+        raise OracleError(status)
+    return int(out[0])
+
+
+def u1_rank(nqubits: int, particle_number: int, words: np.ndarray) -> int:
+    w = np.ascontiguousarray(words, dtype=np.uint64).reshape(-1)
+    if w.size == 0:
+        w = np.zeros(1, np.uint64)
+    out = np.zeros(1, np.uint64)
+    status = _load().oracle_u1_rank(nqubits, particle_number, _p(w, _u64p), _p(out, _u64p))
+    if status:
+        raise OracleError(status)
+    return int(out[0])
+
+
+def u1_unrank(nqubits: int, particle_number: int, index: int) -> np.ndarray:
+    out = np.zeros(max(packed_word_count(nqubits), 1), np.uint64)
+    status = _load().oracle_u1_unrank(nqubits, particle_number, index, _p(out, _u64p))
+    if status:
+        raise OracleError(status)
+    return out[: packed_word_count(nqubits)]
+
+
+def _u1_terms(nqubits: int, x_words: np.ndarray, z_words: np.ndarray, coefficients: np.ndarray):
+    count = int(len(coefficients))
+    width = max(packed_word_count(nqubits), 1)
+    xw = np.zeros((max(count, 1), width), np.uint64)
+    zw = np.zeros((max(count, 1), width), np.uint64)
+    if count and packed_word_count(nqubits):
+        xw[:count] = np.asarray(x_words, np.uint64).reshape(count, -1)
+        zw[:count] = np.asarray(z_words, np.uint64).reshape(count, -1)
+    if packed_word_count(nqubits) == 0:  # n = 0: no words at all
+        xw = np.zeros(1, np.uint64)
+        zw = np.zeros(1, np.uint64)
+    c = np.zeros(max(count, 1), np.complex128)
+    c[:count] = coefficients
+    return count, np.ascontiguousarray(xw), np.ascontiguousarray(zw), c
+
+
+def u1_apply(nqubits: int, particle_number: int, x_words: np.ndarray, z_words: np.ndarray,
+             coefficients: np.ndarray, state: np.ndarray) -> np.ndarray:
+    """Restricted MVP of the canonical operator (packed x/z words, coefficients)."""
+    count, xw, zw, c = _u1_terms(nqubits, x_words, z_words, coefficients)
+    dim = u1_dimension(nqubits, particle_number)
+    x = np.ascontiguousarray(state, dtype=np.complex128)
+    if x.shape != (dim,):
+        raise ValueError(f"state must have shape ({dim},)")
+    out = np.zeros(dim, np.complex128)
+    ls = np.zeros(1, np.uint64)
+    lw = np.zeros(1, np.uint64)
+    status = _load().oracle_u1_apply(nqubits, particle_number, count, _p(xw, _u64p), _p(zw, _u64p),
+                                     _p(c.view(np.float64), _f64p), _p(x.view(np.float64), _f64p),
+                                     _p(out.view(np.float64), _f64p), _p(ls, _u64p), _p(lw, _u64p))
+    if status == 11:
+        raise OracleLeakage(int(ls[0]), int(lw[0]))
+    if status:
+        raise OracleError(status)
+    return out
+
+
+def u1_csr(nqubits: int, particle_number: int, x_words: np.ndarray, z_words: np.ndarray,
+           coefficients: np.ndarray) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Destination-major CSR (indptr, columns, values) of the restricted operator."""
+    count, xw, zw, c = _u1_terms(nqubits, x_words, z_words, coefficients)
+    dim = u1_dimension(nqubits, particle_number)
+    lib = _load()
+    indptr = np.zeros(dim + 1, np.uint64)
+    nnz = np.zeros(1, np.uint64)
+    ls = np.zeros(1, np.uint64)
+    lw = np.zeros(1, np.uint64)
+    one = np.zeros(1, np.uint64)
+    onev = np.zeros(2, np.float64)
+    args = (nqubits, particle_number, count, _p(xw, _u64p), _p(zw, _u64p), _p(c.view(np.float64), _f64p))
+    status = lib.oracle_u1_csr(*args, _p(indptr, _u64p), _p(one, _u64p), _p(onev, _f64p), 0, _p(nnz, _u64p),
+                               _p(ls, _u64p), _p(lw, _u64p))
+    if status == 11:
+        raise OracleLeakage(int(ls[0]), int(lw[0]))
+    if status:
+        raise OracleError(status)
+    m = int(nnz[0])
+    cols = np.zeros(max(m, 1), np.uint64)
+    vals = np.zeros(max(m, 1), np.complex128)
+    status = lib.oracle_u1_csr(*args, _p(indptr, _u64p), _p(cols, _u64p), _p(vals.view(np.float64), _f64p), m,
+                               _p(nnz, _u64p), _p(ls, _u64p), _p(lw, _u64p))
+    if status:
+        raise OracleError(status)
+    return indptr, cols[:m], vals[:m]
+
+
+def number_commutator(nqubits: int, x_words: np.ndarray, z_words: np.ndarray, coefficients: np.ndarray) -> int:
+    """Nonzero commutator words of [H, N] (0 iff H conserves the particle number)."""
+    count, xw, zw, c = _u1_terms(nqubits, x_words, z_words, coefficients)
+    out = np.zeros(1, np.uint64)
+    status = _load().oracle_number_commutator(nqubits, count, _p(xw, _u64p), _p(zw, _u64p),
+                                              _p(c.view(np.float64), _f64p), _p(out, _u64p))
+    if status:
+        raise OracleError(status)
+    return int(out[0])

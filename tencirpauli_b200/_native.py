@@ -31,6 +31,8 @@ TCP_ERR_NON_CANONICAL_TERMS = 7
 TCP_ERR_OVERFLOW = 8
 TCP_ERR_MEMORY_LIMIT = 9
 TCP_ERR_INVALID_SECTOR = 10
+TCP_ERR_SECTOR_LEAKAGE = 11
+TCP_ERR_INVALID_INDEX = 13
 TCP_ERR_INVALID_ARGUMENT = 32
 TCP_ERR_CUDA = 33
 TCP_ERR_DEVICE_TIMEOUT = 34
@@ -83,6 +85,44 @@ SOLVER_SYMBOLS = (
     "tcp_mlp_forward",
     "tcp_mlp_backward_step",
 )
+
+
+# Every symbol include/tcp_sector.h declares.
+SECTOR_SYMBOLS = (
+    "tcp_u1_dimension",
+    "tcp_u1_rank_words",
+    "tcp_u1_unrank_words",
+    "tcp_u1_basis_words",
+    "tcp_pauli_number_commutator",
+    "tcp_u1_plan_create",
+    "tcp_u1_plan_destroy",
+    "tcp_u1_plan_info",
+    "tcp_u1_apply_into_host",
+    "tcp_u1_apply_into_device",
+    "tcp_u1_diagonal_device",
+    "tcp_u1_transition_count",
+    "tcp_u1_csr",
+    "tcp_u1_plan_device_status",
+)
+
+
+class TcpU1PlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("nqubits", ctypes.c_uint32),
+        ("particle_number", ctypes.c_uint32),
+        ("dimension", ctypes.c_uint64),
+        ("term_count", ctypes.c_uint64),
+        ("group_count", ctypes.c_uint64),
+        ("storage", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("transition_count", ctypes.c_int64),
+        ("device_bytes", ctypes.c_uint64),
+        ("estimated_bytes", ctypes.c_uint64),
+        ("complement", ctypes.c_uint32),
+        ("rank_chunks", ctypes.c_uint32),
+        ("tables_in_shared", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
 
 
 class TcpPlanInfo(ctypes.Structure):
@@ -164,6 +204,22 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp, vp]
         lib.tcp_mlp_forward.argtypes = [vp, u32, vp, vp, vp]
         lib.tcp_mlp_backward_step.argtypes = [vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp]
+        lib.tcp_u1_dimension.argtypes = [u32, u32, u64p]
+        lib.tcp_u1_rank_words.argtypes = [u32, u32, u64p, u32, u64p]
+        lib.tcp_u1_unrank_words.argtypes = [u32, u32, u64, u64p, u32]
+        lib.tcp_u1_basis_words.argtypes = [u32, u32, u64p, u64, u64]
+        lib.tcp_pauli_number_commutator.argtypes = [u32, u64, u32, u64p, u64p, f64p, u64p]
+        lib.tcp_u1_plan_create.argtypes = [u32, u32, u64, u32, u64p, u64p, f64p, i32, u64, ctypes.POINTER(vp)]
+        lib.tcp_u1_plan_destroy.argtypes = [vp]
+        lib.tcp_u1_plan_info.argtypes = [vp, ctypes.POINTER(TcpU1PlanInfo)]
+        lib.tcp_u1_apply_into_host.argtypes = [vp, f64p, u64, f64p, u64, u64]
+        lib.tcp_u1_apply_into_device.argtypes = [vp, vp, vp, u64, u32, i32, vp]
+        lib.tcp_u1_diagonal_device.argtypes = [vp, vp, u64, vp]
+        lib.tcp_u1_transition_count.argtypes = [vp, u64p]
+        lib.tcp_u1_csr.argtypes = [vp, u64p, u64p, f64p, u64, u64p]
+        lib.tcp_u1_plan_device_status.argtypes = [vp]
+        for name in SECTOR_SYMBOLS:
+            getattr(lib, name).restype = i32
         for name in SOLVER_SYMBOLS:
             if not name.endswith("_work_bytes"):
                 getattr(lib, name).restype = i32
@@ -454,3 +510,286 @@ class NativeMvpPlan:
     def device_status(self) -> None:
         """Synchronise and raise if a kernel of this plan reported a device error."""
         raise_for_status(self._lib.tcp_mvp_plan_device_status(self._handle))
+
+
+# ----------------------------------------------------------------------------
+# U(1) sector plans (include/tcp_sector.h)
+# ----------------------------------------------------------------------------
+def _terms_arrays(nqubits: int, x_words: np.ndarray, z_words: np.ndarray, coefficients: np.ndarray):
+    count = int(coefficients.shape[0])
+    width = nqubits // 64 + (nqubits % 64 != 0)
+    xw = np.ascontiguousarray(x_words, dtype=np.uint64).reshape(count * width)
+    zw = np.ascontiguousarray(z_words, dtype=np.uint64).reshape(count * width)
+    coeffs = np.ascontiguousarray(coefficients, dtype=np.complex128)
+    if count == 0 or width == 0:  # keep valid pointers
+        xw = np.zeros(max(count * width, 1), np.uint64)
+        zw = np.zeros(max(count * width, 1), np.uint64)
+    if count == 0:
+        coeffs = np.zeros(1, np.complex128)
+    return count, width, xw, zw, coeffs
+
+
+def u1_dimension(nqubits: int, particle_number: int) -> int:
+    out = np.zeros(1, np.uint64)
+    raise_for_status(load_library().tcp_u1_dimension(nqubits, particle_number, _ptr(out, ctypes.c_uint64)))
+    return int(out[0])
+
+
+def u1_rank_words(nqubits: int, particle_number: int, words: np.ndarray) -> int:
+    w = np.ascontiguousarray(words, dtype=np.uint64).reshape(-1)
+    count = int(w.shape[0])
+    buf = w if count else np.zeros(1, np.uint64)
+    out = np.zeros(1, np.uint64)
+    raise_for_status(
+        load_library().tcp_u1_rank_words(
+            nqubits, particle_number, _ptr(buf, ctypes.c_uint64), count, _ptr(out, ctypes.c_uint64)
+        )
+    )
+    return int(out[0])
+
+
+def u1_unrank_words(nqubits: int, particle_number: int, index: int) -> np.ndarray:
+    width = nqubits // 64 + (nqubits % 64 != 0)
+    out = np.zeros(max(width, 1), np.uint64)
+    if index < 0 or index > U64_MAX:
+        raise IndexError("restricted basis index is out of range")
+    raise_for_status(
+        load_library().tcp_u1_unrank_words(nqubits, particle_number, index, _ptr(out, ctypes.c_uint64), width)
+    )
+    return out[:width]
+
+
+def u1_basis_words(nqubits: int, particle_number: int, max_bytes: int) -> Tuple[int, int, np.ndarray]:
+    """``u1_basis_words`` (symmetry.rs:395-436): (dimension, word_count, flat words)."""
+    dim = u1_dimension(nqubits, particle_number)
+    width = 1 if nqubits <= 64 else nqubits // 64 + (nqubits % 64 != 0)
+    if dim * width * 8 > max_bytes:
+        raise MemoryError(f"requested {dim * width * 8} bytes exceeds memory limit {max_bytes}")
+    out = np.zeros(max(dim * width, 1), np.uint64)
+    raise_for_status(
+        load_library().tcp_u1_basis_words(
+            nqubits, particle_number, _ptr(out, ctypes.c_uint64), out.shape[0], min(int(max_bytes), U64_MAX)
+        )
+    )
+    return dim, width, out[: dim * width]
+
+
+def number_commutator(nqubits: int, x_words: np.ndarray, z_words: np.ndarray, coefficients: np.ndarray) -> int:
+    """Nonzero words of [H, N] by the reference's selection rule (0: conserved)."""
+    count, width, xw, zw, coeffs = _terms_arrays(nqubits, x_words, z_words, coefficients)
+    out = np.zeros(1, np.uint64)
+    raise_for_status(
+        load_library().tcp_pauli_number_commutator(
+            nqubits,
+            count,
+            width,
+            _ptr(xw, ctypes.c_uint64),
+            _ptr(zw, ctypes.c_uint64),
+            _ptr(coeffs.view(np.float64), ctypes.c_double),
+            _ptr(out, ctypes.c_uint64),
+        )
+    )
+    return int(out[0])
+
+
+def _stream_handle(stream: Any, device: Any) -> int:
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream(device)
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+
+
+class NativeU1Plan:
+    """Execution handle of one device sector plan (mirror of the PyO3
+    ``NativeU1LazyMvpPlan`` / ``NativeU1RestrictedOperator``,
+    ``crates/tencirpauli-native/src/symmetry.rs:122-368``)."""
+
+    native_variant = "qubit"
+
+    def __init__(
+        self,
+        nqubits: int,
+        particle_number: int,
+        x_words: np.ndarray,
+        z_words: np.ndarray,
+        coefficients: np.ndarray,
+        storage: str = "lazy",
+        max_bytes: int = sys.maxsize,
+    ) -> None:
+        lib = load_library()
+        self._lib = lib
+        self._handle = ctypes.c_void_p(None)
+        if storage not in ("lazy", "eager"):
+            raise ValueError("invalid sector: storage must be either 'eager' or 'lazy'")
+        count, width, xw, zw, coeffs = _terms_arrays(nqubits, x_words, z_words, coefficients)
+        handle = ctypes.c_void_p(None)
+        status = lib.tcp_u1_plan_create(
+            nqubits,
+            particle_number,
+            count,
+            width,
+            _ptr(xw, ctypes.c_uint64),
+            _ptr(zw, ctypes.c_uint64),
+            _ptr(coeffs.view(np.float64), ctypes.c_double),
+            TCP_STORAGE_EAGER if storage == "eager" else TCP_STORAGE_LAZY,
+            min(int(max_bytes), U64_MAX),
+            ctypes.byref(handle),
+        )
+        raise_for_status(status)
+        self._handle = handle
+        info = TcpU1PlanInfo()
+        raise_for_status(lib.tcp_u1_plan_info(handle, ctypes.byref(info)))
+        self._info = info
+        self.storage = storage
+
+    def __del__(self) -> None:
+        handle = getattr(self, "_handle", None)
+        try:
+            if handle is not None and handle.value:
+                self._lib.tcp_u1_plan_destroy(handle)
+                self._handle = None
+        except Exception:  # interpreter shutdown
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._handle
+
+    @property
+    def info(self) -> TcpU1PlanInfo:
+        return self._info
+
+    @property
+    def nqubits(self) -> int:
+        return int(self._info.nqubits)
+
+    @property
+    def particle_number(self) -> int:
+        return int(self._info.particle_number)
+
+    @property
+    def dimension(self) -> int:
+        return int(self._info.dimension)
+
+    @property
+    def term_count(self) -> int:
+        return int(self._info.term_count)
+
+    @property
+    def group_count(self) -> int:
+        return int(self._info.group_count)
+
+    @property
+    def estimated_bytes(self) -> int:
+        return int(self._info.estimated_bytes)
+
+    @property
+    def transition_count(self) -> Optional[int]:
+        value = int(self._info.transition_count)
+        return None if value < 0 else value
+
+    def count_transitions(self) -> int:
+        out = np.zeros(1, np.uint64)
+        raise_for_status(self._lib.tcp_u1_transition_count(self._handle, _ptr(out, ctypes.c_uint64)))
+        return int(out[0])
+
+    def apply_into(self, state: np.ndarray, output: np.ndarray, max_bytes: int) -> None:
+        for name, value in (("input", state), ("output", output)):
+            if not isinstance(value, np.ndarray):
+                raise TypeError("apply_into input and output must be NumPy arrays")
+            if value.dtype != np.complex128:
+                raise TypeError("apply_into input and output must have dtype complex128")
+            if value.ndim != 1:
+                raise ValueError(f"apply_into {name} must be one-dimensional")
+            if not value.flags.c_contiguous:
+                raise ValueError(f"apply_into {name} must be C-contiguous")
+        if not output.flags.writeable:
+            raise ValueError("apply_into output must be writable")
+        status = self._lib.tcp_u1_apply_into_host(
+            self._handle,
+            _ptr(state.view(np.float64), ctypes.c_double),
+            state.shape[0],
+            _ptr(output.view(np.float64), ctypes.c_double),
+            output.shape[0],
+            min(int(max_bytes), U64_MAX),
+        )
+        raise_for_status(status)
+
+    def apply(self, state: np.ndarray, max_bytes: int) -> np.ndarray:
+        values = np.ascontiguousarray(state, dtype=np.complex128)
+        if values.ndim != 1 or values.shape[0] != self.dimension:
+            raise ValueError(f"expected structure length {self.dimension}, got {values.shape[0] if values.ndim else 0}")
+        if self.dimension * 16 > max_bytes:
+            raise MemoryError(f"requested {self.dimension * 16} bytes exceeds memory limit {max_bytes}")
+        out = np.empty(self.dimension, dtype=np.complex128)
+        self.apply_into(values, out, max_bytes)
+        return out
+
+    def apply_device(self, x: Any, y: Any, stream: Any = None) -> None:
+        """Apply to torch CUDA tensors of shape (dim,) or (nrhs, dim)."""
+        import torch
+
+        if not (isinstance(x, torch.Tensor) and isinstance(y, torch.Tensor)):
+            raise TypeError("apply_device needs torch tensors")
+        if x.device.type != "cuda" or y.device.type != "cuda":
+            raise ValueError("apply_device needs CUDA tensors")
+        if x.dtype != y.dtype or x.dtype not in (torch.complex128, torch.complex64):
+            raise TypeError("apply_device tensors must both be complex128 or complex64")
+        if x.shape != y.shape or x.ndim not in (1, 2) or x.shape[-1] != self.dimension:
+            raise ValueError(f"apply_device tensors must have shape ({self.dimension},) or (nrhs, {self.dimension})")
+        if not (x.is_contiguous() and y.is_contiguous()):
+            raise ValueError("apply_device tensors must be contiguous")
+        nrhs = 1 if x.ndim == 1 else int(x.shape[0])
+        dtype = TCP_DTYPE_C128 if x.dtype == torch.complex128 else TCP_DTYPE_C64
+        status = self._lib.tcp_u1_apply_into_device(
+            self._handle,
+            ctypes.c_void_p(x.data_ptr()),
+            ctypes.c_void_p(y.data_ptr()),
+            self.dimension,
+            nrhs,
+            dtype,
+            ctypes.c_void_p(_stream_handle(stream, x.device)),
+        )
+        raise_for_status(status)
+
+    def diagonal_device(self, out: Any, stream: Any = None) -> None:
+        import torch
+
+        if out.dtype != torch.complex128 or out.shape != (self.dimension,) or not out.is_contiguous():
+            raise ValueError("diagonal_device needs a contiguous complex128 tensor of length dim")
+        raise_for_status(
+            self._lib.tcp_u1_diagonal_device(
+                self._handle,
+                ctypes.c_void_p(out.data_ptr()),
+                self.dimension,
+                ctypes.c_void_p(_stream_handle(stream, out.device)),
+            )
+        )
+
+    def csr(self, max_bytes: int) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray]:
+        """(dimension, indptr, columns, values): destinations as rows, columns ascending."""
+        nnz = self.count_transitions()
+        dim = self.dimension
+        need = (dim + 1) * 8 + nnz * 24
+        if need > max_bytes:
+            raise MemoryError(f"requested {need} bytes exceeds memory limit {max_bytes}")
+        indptr = np.zeros(dim + 1, np.uint64)
+        cols = np.zeros(max(nnz, 1), np.uint64)
+        vals = np.zeros(max(nnz, 1), np.complex128)
+        got = np.zeros(1, np.uint64)
+        raise_for_status(
+            self._lib.tcp_u1_csr(
+                self._handle,
+                _ptr(indptr, ctypes.c_uint64),
+                _ptr(cols, ctypes.c_uint64),
+                _ptr(vals.view(np.float64), ctypes.c_double),
+                cols.shape[0],
+                _ptr(got, ctypes.c_uint64),
+            )
+        )
+        m = int(got[0])
+        return dim, indptr, cols[:m], vals[:m]
+
+    def device_status(self) -> None:
+        raise_for_status(self._lib.tcp_u1_plan_device_status(self._handle))

@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import sys
 from dataclasses import dataclass
-from typing import Any, Literal, Optional, Sequence
+from typing import Any, Literal, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -199,3 +199,44 @@ class NativeMvpFacade:
         from .integrations.scipy import to_scipy_linear_operator
 
         return to_scipy_linear_operator(self, max_bytes=max_bytes)
+
+
+@dataclass(frozen=True)
+class COOMatrix:
+    """Coordinate arrays of a materialised operator (``hamiltonian.py:109-132``
+    of the reference): ``row``, ``column``, ``data`` of equal length in the
+    producing operator's order, and the logical ``shape``."""
+
+    row: np.ndarray
+    column: np.ndarray
+    data: np.ndarray
+    shape: Tuple[int, int]
+
+    @property
+    def value(self) -> np.ndarray:
+        return self.data
+
+    def to_scipy(self) -> Any:
+        from scipy.sparse import coo_matrix
+
+        return coo_matrix((self.data, (self.row, self.column)), shape=self.shape)
+
+
+@dataclass(frozen=True)
+class CSRMatrix:
+    """Compressed-sparse-row arrays (``hamiltonian.py:135-158`` of the
+    reference): ``indptr``, ``indices``, ``data`` and ``shape``."""
+
+    indptr: np.ndarray
+    indices: np.ndarray
+    data: np.ndarray
+    shape: Tuple[int, int]
+
+    @property
+    def value(self) -> np.ndarray:
+        return self.data
+
+    def to_scipy(self) -> Any:
+        from scipy.sparse import csr_matrix
+
+        return csr_matrix((self.data, self.indices, self.indptr), shape=self.shape)

@@ -107,7 +107,7 @@ def davidson(
     keep = keep or max(nev + block, max_subspace // 2)
 
     if start is None:
-        X = random_state_device(execution.nqubits, seed=seed, dtype=torch.complex64, nrhs=block)
+        X = random_state_device(execution.nqubits, seed=seed, dtype=torch.complex64, nrhs=block, length=n)
     else:
         X = start
     iterations = 0

@@ -262,6 +262,43 @@ class PauliOperator:
 
         return to_scipy_linear_operator(self.native_mvp_plan(max_bytes=max_bytes), max_bytes=max_bytes)
 
+    # -- U(1) sectors (``pauli.py:705-736,803-828`` of the reference) ----------
+    def conserves_particle_number(self) -> bool:
+        """[H, N] == 0 by the reference's selection rule for qubit levels (0, 1)."""
+        return _native.number_commutator(self.nqubits, self._x_words, self._z_words, self._coefficients) == 0
+
+    def restrict_charge(
+        self,
+        sector: Any,
+        *,
+        storage: Literal["lazy", "eager"] = "lazy",
+        max_bytes: Optional[int] = DEFAULT_MAX_BYTES,
+    ) -> Any:
+        """Restrict a number-conserving operator to a ``U1Sector``.
+
+        Only qubit-number sectors are part of this build; general additive
+        charge sectors are not."""
+        from .symmetry import U1Sector, restrict_u1
+
+        if not isinstance(sector, U1Sector):
+            raise TypeError(f"expected U1Sector, got {type(sector).__name__}")
+        return restrict_u1(self, sector, storage=storage, max_bytes=max_bytes)
+
+    def restrict_u1(
+        self,
+        sector: Any,
+        *,
+        storage: Literal["lazy", "eager"] = "lazy",
+        max_bytes: Optional[int] = DEFAULT_MAX_BYTES,
+    ) -> Any:
+        """Deprecated alias of :meth:`restrict_charge` with a ``U1Sector``."""
+        from .symmetry import U1Sector, deprecated_restrict_u1
+
+        validate_max_bytes(max_bytes)
+        if not isinstance(sector, U1Sector):
+            raise TypeError(f"expected U1Sector, got {type(sector).__name__}")
+        return deprecated_restrict_u1(self, sector, storage, max_bytes)
+
 
 _PLAN_FACTORY_TOKEN = object()
 

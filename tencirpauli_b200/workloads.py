@@ -13,7 +13,7 @@ term rows; :class:`~tencirpauli_b200.pauli.PauliOperator` canonicalizes them
 
 from __future__ import annotations
 
-from typing import List, Tuple
+from typing import Optional, List, Tuple
 
 import numpy as np
 
@@ -137,15 +137,18 @@ def random_state(n: int, seed: int = SEED, dtype: type = np.complex128) -> np.nd
     return state.astype(dtype)
 
 
-def random_state_device(n: int, seed: int = SEED, dtype=None, device: str = "cuda", nrhs: int = 0):
-    """The same distribution generated on the device with torch (large n)."""
+def random_state_device(n: int, seed: int = SEED, dtype=None, device: str = "cuda", nrhs: int = 0,
+                        length: Optional[int] = None):
+    """The same distribution generated on the device with torch (large n).
+    ``length`` overrides the 2^n entries (restricted sector states)."""
     import torch
 
     dtype = dtype or torch.complex128
     real = torch.float64 if dtype == torch.complex128 else torch.float32
     gen = torch.Generator(device=device)
     gen.manual_seed(seed)
-    shape = (nrhs, 1 << n) if nrhs else (1 << n,)
+    size = (1 << n) if length is None else int(length)
+    shape = (nrhs, size) if nrhs else (size,)
     re = torch.randn(shape, generator=gen, device=device, dtype=real)
     im = torch.randn(shape, generator=gen, device=device, dtype=real)
     state = torch.complex(re, im)

@@ -34,6 +34,10 @@ def test_library_loads_and_exports_every_declared_symbol() -> None:
     assert set(solver) == set(_native.SOLVER_SYMBOLS)
     for name in solver:
         assert hasattr(lib, name), name
+    sector = _declared_functions("tcp_sector.h")
+    assert set(sector) == set(_native.SECTOR_SYMBOLS)
+    for name in sector:
+        assert hasattr(lib, name), name
     assert lib.tcp_mlp_train_work_bytes() == 296 * 434 * 4
     assert lib.tcp_gram_work_bytes(4, 3) == 296 * 12 * 16
 
