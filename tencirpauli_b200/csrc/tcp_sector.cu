@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -230,40 +231,100 @@ struct U1Dev {
     uint32_t n, k, kp, comp, nchunk, ngroups, nterms, pad;
 };
 
+// The apply kernel's view: only the groups that can map a sector state to a
+// sector state (x != 0 with an even number of flips), masks in the state word
+// type ST (uint32 for n <= 32, else uint64), and the diagonal of the x == 0
+// group evaluated once per plan.
+//
+// Constant groups.  On a source s = b ^ x inside the sector exactly half of
+// the flipped qubits are set, so a term whose z mask meets x in nothing or in
+// all of x has the fixed sign (-1)^{|x|/2 * [z & x == x]} there, and the rest
+// of its z mask (z_out = z & ~x) reads the same bits in s as in the row b.
+// When every term of a group has such a z & x and one common z_out (XX + YY
+// exchange; Jordan-Wigner hopping with one Z string), the group's value is
+// (-1)^{popcount(z_out & b)} * C with C summed once at plan build, in the
+// canonical term order from 0 as the reference sums it -- negating a sum term
+// by term negates it exactly, so the value is bit-identical.  Other groups
+// run the term loop.
+//
+// Fast ranks (n <= 32): rank(s) = H[top] + M[popcount(top)][mid] + L[low]
+// (three levels) or H[s >> L] + L[s & (2^L - 1)] (two levels, no middle):
+// H counts the sector states with a smaller top part, M those with the same
+// top part and a smaller middle part, L ranks the low bits among words of
+// their own weight.
+constexpr uint32_t kGroupConst = 1u << 31;  // ainfo: value is +-C
+constexpr uint32_t kGroupZout = 1u << 30;   // ainfo: sign by popcount(z_out & b)
+constexpr uint32_t kGroupHalf = 0xffffu;    // ainfo: popcount(x) / 2
+
+struct U1Apply {
+    const uint32_t *ftab;  // fast rank tables (rk 2 or 3), else null
+    uint32_t rk, rL, rM, lmask, mmask, h_off, m_off, l_off;
+    size_t ftab_bytes;
+    const void *ax;        // ST[ga]: x masks
+    const uint32_t *ainfo; // [ga]: half | kGroupConst | kGroupZout
+    const void *azo;       // ST[ga]: z_out of constant groups
+    const double2 *ac;     // [ga]: C of constant groups
+    const float2 *acf;     // [ga]: C rounded to FP32
+    const uint32_t *at;    // [ga + 1]: term offsets (empty for constant groups)
+    const void *az;        // ST[ta]: term z masks
+    const double2 *aw;     // [ta]
+    const float2 *awf;     // [ta]
+    const double2 *diag;   // [dim] or null when there is no x == 0 group
+    uint32_t ga, ta;
+};
+
 template <typename R> struct Cplx;
 template <> struct Cplx<double> { using T = double2; };
 template <> struct Cplx<float> { using T = float2; };
 
+template <typename ST> __device__ __forceinline__ uint32_t popc_t(ST v);
+template <> __device__ __forceinline__ uint32_t popc_t<uint32_t>(uint32_t v) { return static_cast<uint32_t>(__popc(v)); }
+template <> __device__ __forceinline__ uint32_t popc_t<uint64_t>(uint64_t v) { return static_cast<uint32_t>(__popcll(v)); }
+
+// Rank of a sector state: one table load per 8-bit chunk, top chunk first,
+// `a` counting the ones above the chunk.  IT is wide enough for the dimension.
+template <typename ST, typename IT>
+__device__ __forceinline__ uint64_t rank_t(ST s, const IT *__restrict__ tab, const U1Dev &p) {
+    const ST a_state = p.comp ? static_cast<ST>(~s & static_cast<ST>(p.mask)) : s;
+    IT r = 0;
+    uint32_t a = 0;
+    const uint32_t row = (p.kp + 1) * 256u;
+#pragma unroll
+    for (int c = static_cast<int>(sizeof(ST)) - 1; c >= 0; --c) {
+        if (c < static_cast<int>(p.nchunk)) {
+            const uint32_t v = static_cast<uint32_t>(a_state >> (8 * c)) & 255u;
+            r += tab[static_cast<uint32_t>(c) * row + a * 256u + v];
+            a += __popc(v);
+        }
+    }
+    return p.comp ? (p.dim - 1 - static_cast<uint64_t>(r)) : static_cast<uint64_t>(r);
+}
+
 template <typename IT>
 __device__ __forceinline__ uint64_t rank_state(uint64_t s, const IT *__restrict__ tab, const U1Dev &p) {
-    uint64_t a_state = p.comp ? (~s & p.mask) : s;
-    uint64_t r = 0;
-    uint32_t a = 0;
-    const uint32_t row = p.kp + 1;
-    for (int c = static_cast<int>(p.nchunk) - 1; c >= 0; --c) {
-        const uint32_t v = static_cast<uint32_t>(a_state >> (8 * c)) & 255u;
-        r += tab[(static_cast<uint32_t>(c) * row + a) * 256u + v];
-        a += __popc(v);
-    }
-    return p.comp ? (p.dim - 1 - r) : r;
+    return rank_t<uint64_t, IT>(s, tab, p);
 }
 
 // Stage the rank tables, groups and terms in shared memory (16-byte aligned
 // pieces, copied with 16-byte vector loads).
-struct U1Smem {
-    size_t tab, gx, gt, tz, tw, total;
-};
-
 __host__ __device__ inline size_t al16(size_t v) { return (v + 15) & ~size_t(15); }
 
-__host__ __device__ inline U1Smem u1_smem_layout(size_t tab_bytes, uint32_t G, uint32_t T, size_t wbytes) {
-    U1Smem s;
+struct U1ApplySmem {
+    size_t tab, ax, ai, azo, ac, at, az, aw, total;
+};
+
+__host__ __device__ inline U1ApplySmem u1_apply_layout(size_t tab_bytes, uint32_t G, uint32_t T, size_t sbytes,
+                                                       size_t wbytes) {
+    U1ApplySmem s;
     s.tab = 0;
-    s.gx = al16(tab_bytes);
-    s.gt = s.gx + al16(8ull * G);
-    s.tz = s.gt + al16(4ull * (G + 1));
-    s.tw = s.tz + al16(8ull * T);
-    s.total = s.tw + al16(wbytes * T);
+    s.ax = al16(tab_bytes);
+    s.ai = s.ax + al16(sbytes * G);
+    s.azo = s.ai + al16(4ull * G);
+    s.ac = s.azo + al16(sbytes * G);
+    s.at = s.ac + al16(wbytes * G);
+    s.az = s.at + al16(4ull * (G + 1));
+    s.aw = s.az + al16(sbytes * T);
+    s.total = s.aw + al16(wbytes * T);
     return s;
 }
 
@@ -276,82 +337,163 @@ __device__ __forceinline__ void copy16(unsigned char *dst, const void *src, size
     if (threadIdx.x < rem) dst[n16 * 16 + threadIdx.x] = static_cast<const unsigned char *>(src)[n16 * 16 + threadIdx.x];
 }
 
-template <typename R> __device__ __forceinline__ const typename Cplx<R>::T *weights_of(const U1Dev &p);
-template <> __device__ __forceinline__ const double2 *weights_of<double>(const U1Dev &p) { return p.tw; }
-template <> __device__ __forceinline__ const float2 *weights_of<float>(const U1Dev &p) { return p.twf; }
 
-// y = H_sector x.  One output row per thread, grid-stride over rows.
-template <typename R, typename BT, typename IT, bool SM>
-__global__ void __launch_bounds__(kU1Threads) k_u1_apply(U1Dev p, size_t tab_bytes,
+template <typename R> struct ApplyW;
+template <> struct ApplyW<double> {
+    static __device__ __forceinline__ const double2 *terms(const U1Apply &a) { return a.aw; }
+    static __device__ __forceinline__ const double2 *consts(const U1Apply &a) { return a.ac; }
+};
+template <> struct ApplyW<float> {
+    static __device__ __forceinline__ const float2 *terms(const U1Apply &a) { return a.awf; }
+    static __device__ __forceinline__ const float2 *consts(const U1Apply &a) { return a.acf; }
+};
+
+// Rank of a sector state for rank kind RK (2, 3: fast tables; 0: 8-bit chunks).
+template <int RK, typename ST, typename IT>
+__device__ __forceinline__ uint64_t rank_any(ST s, const IT *__restrict__ tab, const U1Dev &p, const U1Apply &a) {
+    if constexpr (RK == 2) {
+        const uint32_t v = static_cast<uint32_t>(s);
+        return static_cast<uint64_t>(tab[a.h_off + (v >> a.rL)] + tab[a.l_off + (v & a.lmask)]);
+    } else if constexpr (RK == 3) {
+        const uint32_t v = static_cast<uint32_t>(s);
+        const uint32_t top = v >> (a.rM + a.rL);
+        const uint32_t mid = (v >> a.rL) & a.mmask;
+        return static_cast<uint64_t>(tab[a.h_off + top] + tab[a.m_off + (static_cast<uint32_t>(__popc(top)) << a.rM) + mid] +
+                                     tab[a.l_off + (v & a.lmask)]);
+    } else {
+        return rank_t<ST, IT>(s, tab, p);
+    }
+}
+
+// y = H_sector x.  One output row per thread, grid-stride over rows.  Row i
+// starts from diag[i] * x[i]; the other groups run in blocks of U: every
+// group of a block is tested (popcount(b & x) == |x| / 2), valued and ranked,
+// then the U gathers are issued back to back and accumulated in group order.
+// A skipped group (source outside the sector, or a value of exactly zero)
+// loads the thread's own row, which is always valid, and is not added.
+template <typename R, typename ST, typename IT, int RK, bool SM, bool DIAG>
+__global__ void __launch_bounds__(kU1Threads) k_u1_apply(U1Dev p, U1Apply a, size_t tab_bytes,
                                                          const typename Cplx<R>::T *__restrict__ x,
                                                          typename Cplx<R>::T *__restrict__ y) {
     using C = typename Cplx<R>::T;
+    constexpr int U = 4;
     extern __shared__ __align__(16) unsigned char sm[];
     const IT *tab;
-    const uint64_t *gx;
-    const uint32_t *gt;
-    const uint64_t *tz;
-    const C *tw;
+    const ST *ax;
+    const uint32_t *ai;
+    const ST *azo;
+    const C *ac;
+    const uint32_t *at;
+    const ST *az;
+    const C *aw;
+    const void *tab_src = RK ? static_cast<const void *>(a.ftab) : p.tab;
     if (SM) {
-        const U1Smem L = u1_smem_layout(tab_bytes, p.ngroups, p.nterms, sizeof(C));
-        copy16(sm + L.tab, p.tab, tab_bytes);
-        copy16(sm + L.gx, p.gx, 8ull * p.ngroups);
-        copy16(sm + L.gt, p.gt, 4ull * (p.ngroups + 1));
-        copy16(sm + L.tz, p.tz, 8ull * p.nterms);
-        copy16(sm + L.tw, weights_of<R>(p), sizeof(C) * p.nterms);
+        const U1ApplySmem L = u1_apply_layout(tab_bytes, a.ga, a.ta, sizeof(ST), sizeof(C));
+        copy16(sm + L.tab, tab_src, tab_bytes);
+        copy16(sm + L.ax, a.ax, sizeof(ST) * a.ga);
+        copy16(sm + L.ai, a.ainfo, 4ull * a.ga);
+        copy16(sm + L.azo, a.azo, sizeof(ST) * a.ga);
+        copy16(sm + L.ac, ApplyW<R>::consts(a), sizeof(C) * a.ga);
+        copy16(sm + L.at, a.at, 4ull * (a.ga + 1));
+        copy16(sm + L.az, a.az, sizeof(ST) * a.ta);
+        copy16(sm + L.aw, ApplyW<R>::terms(a), sizeof(C) * a.ta);
         __syncthreads();
         tab = reinterpret_cast<const IT *>(sm + L.tab);
-        gx = reinterpret_cast<const uint64_t *>(sm + L.gx);
-        gt = reinterpret_cast<const uint32_t *>(sm + L.gt);
-        tz = reinterpret_cast<const uint64_t *>(sm + L.tz);
-        tw = reinterpret_cast<const C *>(sm + L.tw);
+        ax = reinterpret_cast<const ST *>(sm + L.ax);
+        ai = reinterpret_cast<const uint32_t *>(sm + L.ai);
+        azo = reinterpret_cast<const ST *>(sm + L.azo);
+        ac = reinterpret_cast<const C *>(sm + L.ac);
+        at = reinterpret_cast<const uint32_t *>(sm + L.at);
+        az = reinterpret_cast<const ST *>(sm + L.az);
+        aw = reinterpret_cast<const C *>(sm + L.aw);
     } else {
-        tab = static_cast<const IT *>(p.tab);
-        gx = p.gx;
-        gt = p.gt;
-        tz = p.tz;
-        tw = weights_of<R>(p);
+        tab = static_cast<const IT *>(tab_src);
+        ax = static_cast<const ST *>(a.ax);
+        ai = a.ainfo;
+        azo = static_cast<const ST *>(a.azo);
+        ac = ApplyW<R>::consts(a);
+        at = a.at;
+        az = static_cast<const ST *>(a.az);
+        aw = ApplyW<R>::terms(a);
     }
-    const BT *basis = static_cast<const BT *>(p.basis);
+    const ST *basis = static_cast<const ST *>(p.basis);
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.dim; i += stride) {
-        const uint64_t b = static_cast<uint64_t>(basis[i]);
-        R ar = 0, ai = 0, cr = 0, ci = 0;  // cr, ci: Kahan compensation (FP32 only)
-        for (uint32_t g = 0; g < p.ngroups; ++g) {
-            const uint64_t s = b ^ gx[g];
-            if (static_cast<uint32_t>(__popcll(s)) != p.k) continue;
-            R vr = 0, vi = 0;
-            const uint32_t te = gt[g + 1];
-            for (uint32_t t = gt[g]; t < te; ++t) {
-                const C w = tw[t];
-                if (__popcll(tz[t] & s) & 1) {
-                    vr -= w.x;
-                    vi -= w.y;
-                } else {
-                    vr += w.x;
-                    vi += w.y;
-                }
+        const ST b = basis[i];
+        R ar = 0, ai_ = 0, cr = 0, ci = 0;  // cr, ci: Kahan compensation (FP32 only)
+        if (DIAG) {
+            const double2 d = a.diag[i];
+            const C xv = x[i];
+            const R dr = static_cast<R>(d.x), di = static_cast<R>(d.y);
+            if (dr != R(0) || di != R(0)) {
+                ar = dr * xv.x - di * xv.y;
+                ai_ = dr * xv.y + di * xv.x;
             }
-            if (vr == R(0) && vi == R(0)) continue;
-            const uint64_t j = (s == b) ? i : rank_state<IT>(s, tab, p);
-            const C xv = x[j];
-            const R pr = vr * xv.x - vi * xv.y;
-            const R pi = vr * xv.y + vi * xv.x;
-            if (sizeof(R) == 8) {
-                ar += pr;
-                ai += pi;
-            } else {
-                const R yr = pr - cr, yi = pi - ci;
-                const R tr = ar + yr, ti = ai + yi;
-                cr = (tr - ar) - yr;
-                ci = (ti - ai) - yi;
-                ar = tr;
-                ai = ti;
+        }
+        for (uint32_t g0 = 0; g0 < a.ga; g0 += U) {
+            uint64_t j[U];
+            R vr[U], vi[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t g = g0 + u;
+                vr[u] = 0;
+                vi[u] = 0;
+                j[u] = i;
+                if (g >= a.ga) continue;
+                const ST xm = ax[g];
+                const uint32_t info = ai[g];
+                if (popc_t<ST>(b & xm) != (info & kGroupHalf)) continue;
+                const ST s = b ^ xm;
+                R wr = 0, wi = 0;
+                if (info & kGroupConst) {
+                    const C c = ac[g];
+                    wr = c.x;
+                    wi = c.y;
+                    if ((info & kGroupZout) && (popc_t<ST>(azo[g] & b) & 1u)) {
+                        wr = -wr;
+                        wi = -wi;
+                    }
+                } else {
+                    const uint32_t te = at[g + 1];
+                    for (uint32_t t = at[g]; t < te; ++t) {
+                        const C w = aw[t];
+                        if (popc_t<ST>(az[t] & s) & 1u) {
+                            wr -= w.x;
+                            wi -= w.y;
+                        } else {
+                            wr += w.x;
+                            wi += w.y;
+                        }
+                    }
+                }
+                vr[u] = wr;
+                vi[u] = wi;
+                if (wr != R(0) || wi != R(0)) j[u] = rank_any<RK, ST, IT>(s, tab, p, a);
+            }
+            C xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = x[j[u]];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (vr[u] == R(0) && vi[u] == R(0)) continue;
+                const R pr = vr[u] * xv[u].x - vi[u] * xv[u].y;
+                const R pi = vr[u] * xv[u].y + vi[u] * xv[u].x;
+                if (sizeof(R) == 8) {
+                    ar += pr;
+                    ai_ += pi;
+                } else {
+                    const R yr = pr - cr, yi = pi - ci;
+                    const R tr = ar + yr, ti = ai_ + yi;
+                    cr = (tr - ar) - yr;
+                    ci = (ti - ai_) - yi;
+                    ar = tr;
+                    ai_ = ti;
+                }
             }
         }
         C out;
         out.x = ar;
-        out.y = ai;
+        out.y = ai_;
         y[i] = out;
     }
 }
@@ -493,6 +635,7 @@ struct tcp_u1_plan {
     size_t tab_bytes = 0, smem_c128 = 0, smem_c64 = 0;
     U1Terms terms;
     U1Dev dev{};
+    U1Apply app{};
     void *block = nullptr;
     size_t block_bytes = 0;
     mutable std::mutex ws_mutex;
@@ -557,35 +700,48 @@ std::string bytes_str(unsigned __int128 v) {
     return v >> 64 ? std::string("more than 2^64") : std::to_string(static_cast<uint64_t>(v));
 }
 
-template <typename R, typename BT, typename IT>
-int launch_apply_t(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
+template <typename R, typename ST, typename IT, int RK, bool SM, bool DIAG>
+int launch_apply_v(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
     using C = typename Cplx<R>::T;
-    const size_t smem = sizeof(R) == 8 ? p->smem_c128 : p->smem_c64;
+    auto kern = k_u1_apply<R, ST, IT, RK, SM, DIAG>;
     int grid = grid_for(p->dim);
-    if (p->smem) {
+    size_t smem = 0;
+    const size_t tab_bytes = RK ? p->app.ftab_bytes : p->tab_bytes;
+    if (SM) {
         // one wave of resident CTAs: each CTA stages the tables once
-        auto kern = k_u1_apply<R, BT, IT, true>;
+        smem = sizeof(R) == 8 ? p->smem_c128 : p->smem_c64;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
         int per_sm = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kU1Threads, smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         grid = std::min<int>(grid, std::max(per_sm, 1) * std::max(g_sms, 1));
-        kern<<<grid, kU1Threads, smem, s>>>(p->dev, p->tab_bytes, static_cast<const C *>(x), static_cast<C *>(y));
-    } else {
-        k_u1_apply<R, BT, IT, false><<<grid, kU1Threads, 0, s>>>(p->dev, p->tab_bytes, static_cast<const C *>(x),
-                                                                  static_cast<C *>(y));
     }
+    kern<<<grid, kU1Threads, smem, s>>>(p->dev, p->app, tab_bytes, static_cast<const C *>(x), static_cast<C *>(y));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "sector MVP kernel launch");
+}
+
+template <typename R, typename ST, typename IT, int RK>
+int launch_apply_t(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
+    const bool diag = p->app.diag != nullptr;
+    if (p->smem) {
+        return diag ? launch_apply_v<R, ST, IT, RK, true, true>(p, x, y, s)
+                    : launch_apply_v<R, ST, IT, RK, true, false>(p, x, y, s);
+    }
+    return diag ? launch_apply_v<R, ST, IT, RK, false, true>(p, x, y, s)
+                : launch_apply_v<R, ST, IT, RK, false, false>(p, x, y, s);
 }
 
 template <typename R>
 int launch_apply(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
     if (p->dim == 0) return TCP_OK;
-    if (p->basis32) return launch_apply_t<R, uint32_t, uint32_t>(p, x, y, s);
-    if (p->index32) return launch_apply_t<R, uint64_t, uint32_t>(p, x, y, s);
-    return launch_apply_t<R, uint64_t, uint64_t>(p, x, y, s);
+    if (p->basis32) {
+        return p->app.rk == 2 ? launch_apply_t<R, uint32_t, uint32_t, 2>(p, x, y, s)
+                              : launch_apply_t<R, uint32_t, uint32_t, 3>(p, x, y, s);
+    }
+    if (p->index32) return launch_apply_t<R, uint64_t, uint32_t, 0>(p, x, y, s);
+    return launch_apply_t<R, uint64_t, uint64_t, 0>(p, x, y, s);
 }
 
 int count_transitions(const tcp_u1_plan *p, uint64_t *row_counts, uint64_t &total, cudaStream_t s) {
@@ -665,6 +821,129 @@ int upload(tcp_u1_plan *p) {
     if (p->index32) tab32.assign(tab.begin(), tab.end());
     std::vector<float> twf(2 * static_cast<size_t>(T));
     for (size_t i = 0; i < twf.size(); ++i) twf[i] = static_cast<float>(t.tw[i]);
+    // apply view: groups with x != 0 and an even number of flips
+    const size_t ssz = p->basis32 ? 4 : 8;
+    std::vector<unsigned char> ax, azo, az;
+    std::vector<uint32_t> ainfo, at(1, 0);
+    std::vector<double> ac, aw;
+    std::vector<float> acf, awf;
+    auto put = [&](std::vector<unsigned char> &v, uint64_t m) {
+        const size_t o = v.size();
+        v.resize(o + ssz);
+        if (ssz == 4) {
+            const uint32_t m32 = static_cast<uint32_t>(m);
+            std::memcpy(v.data() + o, &m32, 4);
+        } else {
+            std::memcpy(v.data() + o, &m, 8);
+        }
+    };
+    for (uint32_t g = 0; g < G; ++g) {
+        const uint64_t x = t.gx[g];
+        const uint32_t w = static_cast<uint32_t>(__builtin_popcountll(x));
+        if (x == 0 || (w & 1)) continue;
+        const uint32_t tb = t.gt[g], te = t.gt[g + 1];
+        bool constant = true;
+        const uint64_t zout = t.tz[tb] & ~x;
+        for (uint32_t q = tb; q < te && constant; ++q) {
+            const uint64_t zin = t.tz[q] & x;
+            constant = (zin == 0 || zin == x) && (t.tz[q] & ~x) == zout;
+        }
+        put(ax, x);
+        put(azo, zout);
+        uint32_t info = w / 2;
+        double cr = 0.0, ci = 0.0;
+        if (constant) {
+            // the group value where popcount(z_out & b) is even, summed from 0
+            // in canonical term order as aggregate_source sums it
+            for (uint32_t q = tb; q < te; ++q) {
+                const bool neg = ((t.tz[q] & x) == x) && ((w / 2) & 1);
+                if (neg) {
+                    cr -= t.tw[2 * q];
+                    ci -= t.tw[2 * q + 1];
+                } else {
+                    cr += t.tw[2 * q];
+                    ci += t.tw[2 * q + 1];
+                }
+            }
+            info |= kGroupConst | (zout ? kGroupZout : 0u);
+        } else {
+            for (uint32_t q = tb; q < te; ++q) {
+                put(az, t.tz[q]);
+                aw.push_back(t.tw[2 * q]);
+                aw.push_back(t.tw[2 * q + 1]);
+                awf.push_back(twf[2 * q]);
+                awf.push_back(twf[2 * q + 1]);
+            }
+        }
+        ainfo.push_back(info);
+        ac.push_back(cr);
+        ac.push_back(ci);
+        acf.push_back(static_cast<float>(cr));
+        acf.push_back(static_cast<float>(ci));
+        at.push_back(static_cast<uint32_t>(aw.size() / 2));
+    }
+    const uint32_t GA = static_cast<uint32_t>(ainfo.size()), TA = at.back();
+    const bool has_diag = t.gzero >= 0;
+    // fast rank tables (n <= 32): two levels up to 24 qubits, else three
+    std::vector<uint32_t> ftab;
+    U1Apply fast{};
+    if (p->basis32) {
+        const uint32_t n = p->n, k = p->k;
+        uint32_t T_ = 0, M_ = 0, L_ = 0;
+        if (n <= 24) {
+            L_ = n / 2;
+            T_ = n - L_;
+        } else {
+            size_t best = ~size_t(0);
+            for (uint32_t a = 1; a + 2 <= n; ++a)
+                for (uint32_t b = 1; a + b + 1 <= n; ++b) {
+                    const uint32_t c = n - a - b;
+                    const size_t e = (size_t(1) << a) + (std::min(k, a) + 1) * (size_t(1) << b) + (size_t(1) << c);
+                    if (e < best) {
+                        best = e;
+                        T_ = a;
+                        M_ = b;
+                        L_ = c;
+                    }
+                }
+        }
+        const uint32_t lowbits = M_ + L_;  // bits below the top part
+        std::vector<uint32_t> H(size_t(1) << T_), Lr(size_t(1) << L_), Mid;
+        {
+            std::vector<uint32_t> seen(L_ + 1, 0);
+            for (uint32_t v = 0; v < (1u << L_); ++v) Lr[v] = seen[__builtin_popcount(v)]++;
+            uint64_t acc = 0;
+            for (uint32_t h = 0; h < (1u << T_); ++h) {
+                H[h] = static_cast<uint32_t>(acc);
+                const int need = static_cast<int>(k) - __builtin_popcount(h);
+                if (need >= 0 && static_cast<uint32_t>(need) <= lowbits) acc += choose[lowbits * 65 + need];
+            }
+        }
+        if (M_) {
+            const uint32_t rows = std::min(k, T_) + 1;
+            Mid.assign(size_t(rows) << M_, 0);
+            for (uint32_t a = 0; a < rows; ++a) {
+                uint64_t acc = 0;
+                for (uint32_t v = 0; v < (1u << M_); ++v) {
+                    Mid[(size_t(a) << M_) + v] = static_cast<uint32_t>(acc);
+                    const int need = static_cast<int>(k) - static_cast<int>(a) - __builtin_popcount(v);
+                    if (need >= 0 && static_cast<uint32_t>(need) <= L_) acc += choose[L_ * 65 + need];
+                }
+            }
+        }
+        fast.rk = M_ ? 3 : 2;
+        fast.rL = L_;
+        fast.rM = M_;
+        fast.lmask = L_ ? ((1u << L_) - 1) : 0u;
+        fast.mmask = M_ ? ((1u << M_) - 1) : 0u;
+        fast.h_off = 0;
+        fast.m_off = static_cast<uint32_t>(H.size());
+        fast.l_off = static_cast<uint32_t>(H.size() + Mid.size());
+        ftab.insert(ftab.end(), H.begin(), H.end());
+        ftab.insert(ftab.end(), Mid.begin(), Mid.end());
+        ftab.insert(ftab.end(), Lr.begin(), Lr.end());
+        fast.ftab_bytes = 4 * ftab.size();
+    }
     Piece pieces[] = {
         {choose.data(), choose.size() * 8, 0},
         {p->index32 ? static_cast<const void *>(tab32.data()) : tab.data(), p->tab_bytes, 0},
@@ -674,6 +953,17 @@ int upload(tcp_u1_plan *p) {
         {t.tw.data(), 16ull * T, 0},
         {twf.data(), 8ull * T, 0},
         {nullptr, bsz * p->dim, 0},  // basis, generated on the device
+        {ax.data(), ax.size(), 0},
+        {ainfo.data(), 4ull * GA, 0},
+        {azo.data(), azo.size(), 0},
+        {ac.data(), 8ull * ac.size(), 0},
+        {acf.data(), 4ull * acf.size(), 0},
+        {at.data(), 4ull * (GA + 1), 0},
+        {az.data(), az.size(), 0},
+        {aw.data(), 8ull * aw.size(), 0},
+        {awf.data(), 4ull * awf.size(), 0},
+        {nullptr, has_diag ? 16 * p->dim : 0, 0},  // diagonal, evaluated on the device
+        {ftab.data(), 4ull * ftab.size(), 0},
     };
     size_t off = 0;
     for (auto &pc : pieces) {
@@ -716,6 +1006,21 @@ int upload(tcp_u1_plan *p) {
     d.nchunk = p->nchunk;
     d.ngroups = G;
     d.nterms = T;
+    U1Apply &ap = p->app;
+    ap = fast;
+    ap.ax = base + pieces[8].off;
+    ap.ainfo = reinterpret_cast<const uint32_t *>(base + pieces[9].off);
+    ap.azo = base + pieces[10].off;
+    ap.ac = reinterpret_cast<const double2 *>(base + pieces[11].off);
+    ap.acf = reinterpret_cast<const float2 *>(base + pieces[12].off);
+    ap.at = reinterpret_cast<const uint32_t *>(base + pieces[13].off);
+    ap.az = base + pieces[14].off;
+    ap.aw = reinterpret_cast<const double2 *>(base + pieces[15].off);
+    ap.awf = reinterpret_cast<const float2 *>(base + pieces[16].off);
+    ap.diag = has_diag ? reinterpret_cast<const double2 *>(base + pieces[17].off) : nullptr;
+    ap.ftab = p->basis32 ? reinterpret_cast<const uint32_t *>(base + pieces[18].off) : nullptr;
+    ap.ga = GA;
+    ap.ta = TA;
     // basis generation
     const uint32_t rows_per_thread = 64;
     const uint64_t threads = (p->dim + rows_per_thread - 1) / rows_per_thread;
@@ -723,15 +1028,23 @@ int upload(tcp_u1_plan *p) {
     if (p->basis32) k_u1_basis<uint32_t><<<blocks, kU1Threads>>>(d, rows_per_thread, static_cast<uint32_t *>(const_cast<void *>(d.basis)));
     else k_u1_basis<uint64_t><<<blocks, kU1Threads>>>(d, rows_per_thread, static_cast<uint64_t *>(const_cast<void *>(d.basis)));
     e = cudaGetLastError();
+    if (e == cudaSuccess && has_diag) {
+        const int grid = grid_for(p->dim);
+        double2 *diag = reinterpret_cast<double2 *>(base + pieces[17].off);
+        if (p->basis32) k_u1_diag<uint32_t><<<grid, kU1Threads>>>(d, t.gzero, diag);
+        else k_u1_diag<uint64_t><<<grid, kU1Threads>>>(d, t.gzero, diag);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         cudaFree(block);
         p->block = nullptr;
-        return cuda_fail(e, "generating the sector basis");
+        return cuda_fail(e, "generating the sector basis and diagonal");
     }
-    // shared-memory staging
-    p->smem_c128 = u1_smem_layout(p->tab_bytes, G, T, 16).total;
-    p->smem_c64 = u1_smem_layout(p->tab_bytes, G, T, 8).total;
+    // shared-memory staging of the apply view
+    const size_t apply_tab = p->basis32 ? ap.ftab_bytes : p->tab_bytes;
+    p->smem_c128 = u1_apply_layout(apply_tab, GA, TA, ssz, 16).total;
+    p->smem_c64 = u1_apply_layout(apply_tab, GA, TA, ssz, 8).total;
     p->smem = p->smem_c128 <= kU1SmemMax;
     return TCP_OK;
 }
@@ -1038,11 +1351,10 @@ extern "C" int tcp_u1_diagonal_device(const tcp_u1_plan *plan, void *d_diag, uin
     if (len != plan->dim) return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH, "expected structure length " + std::to_string(plan->dim) + ", got " + std::to_string(len));
     if (d_diag == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int grid = grid_for(plan->dim);
-    if (plan->basis32) k_u1_diag<uint32_t><<<grid, kU1Threads, 0, s>>>(plan->dev, plan->terms.gzero, static_cast<double2 *>(d_diag));
-    else k_u1_diag<uint64_t><<<grid, kU1Threads, 0, s>>>(plan->dev, plan->terms.gzero, static_cast<double2 *>(d_diag));
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "sector diagonal kernel launch");
+    // the plan holds the diagonal of its x == 0 group (zero when it has none)
+    cudaError_t e = plan->app.diag ? cudaMemcpyAsync(d_diag, plan->app.diag, 16 * plan->dim, cudaMemcpyDeviceToDevice, s)
+                                   : cudaMemsetAsync(d_diag, 0, 16 * plan->dim, s);
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "copying the sector diagonal");
 }
 
 extern "C" int tcp_u1_transition_count(const tcp_u1_plan *plan, uint64_t *out_count) {
