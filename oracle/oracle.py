@@ -23,6 +23,7 @@ U(1) sector items (``oracle/u1_oracle.c``, paths in ``sector.rs``):
 * :func:`u1_apply`           -- ``U1LazyMvpPlan::apply_into`` (``:579-643``)
 * :func:`u1_csr`             -- ``U1RestrictedOperator::new`` / ``csr`` (``:345-431``)
 * :func:`number_commutator`  -- ``operator.rs:396-444`` with levels (0, 1)
+* :func:`u1_apply_rows`      -- selected rows of the restricted MVP (CPU baseline sample)
 """
 
 from __future__ import annotations
@@ -74,8 +75,9 @@ def _load() -> ctypes.CDLL:
         lib.oracle_u1_apply.argtypes = [u32, u32, u64, _u64p, _u64p, _f64p, _f64p, _f64p, _u64p, _u64p]
         lib.oracle_u1_csr.argtypes = [u32, u32, u64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p, u64, _u64p, _u64p, _u64p]
         lib.oracle_number_commutator.argtypes = [u32, u64, _u64p, _u64p, _f64p, _u64p]
+        lib.oracle_u1_apply_rows.argtypes = [u32, u32, u64, _u64p, _u64p, _f64p, _f64p, u64, _u64p, _f64p, i32]
         for name in ("oracle_u1_dimension", "oracle_u1_rank", "oracle_u1_unrank", "oracle_u1_apply",
-                     "oracle_u1_csr", "oracle_number_commutator"):
+                     "oracle_u1_csr", "oracle_number_commutator", "oracle_u1_apply_rows"):
             getattr(lib, name).restype = i32
         for name in (
             "oracle_encode_codes",
@@ -410,3 +412,19 @@ def number_commutator(nqubits: int, x_words: np.ndarray, z_words: np.ndarray, co
     if status:
         raise OracleError(status)
     return int(out[0])
+
+
+def u1_apply_rows(nqubits: int, particle_number: int, x_words: np.ndarray, z_words: np.ndarray,
+                  coefficients: np.ndarray, state: np.ndarray, rows: np.ndarray, threads: int = 0) -> np.ndarray:
+    """Rows ``rows`` (restricted indices) of the restricted MVP, pulled from their sources."""
+    count, xw, zw, c = _u1_terms(nqubits, x_words, z_words, coefficients)
+    x = np.ascontiguousarray(state, dtype=np.complex128)
+    r = np.ascontiguousarray(rows, dtype=np.uint64)
+    out = np.zeros(max(len(r), 1), np.complex128)
+    status = _load().oracle_u1_apply_rows(nqubits, particle_number, count, _p(xw, _u64p), _p(zw, _u64p),
+                                          _p(c.view(np.float64), _f64p), _p(x.view(np.float64), _f64p), len(r),
+                                          _p(r if len(r) else np.zeros(1, np.uint64), _u64p),
+                                          _p(out.view(np.float64), _f64p), threads or max_threads())
+    if status:
+        raise OracleError(status)
+    return out[: len(r)]

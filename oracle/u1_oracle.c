@@ -395,3 +395,62 @@ int oracle_number_commutator(uint32_t n, uint64_t count, const uint64_t *xw, con
     free(c);
     return 0;
 }
+
+/* Selected destination rows of the restricted MVP, pulled from their sources
+ * (the destination-major reading of aggregate_source, used to time the CPU
+ * baseline on a row sample).  rows: restricted indices; out[2*i] receives
+ * row rows[i].  Leakage is not checked here.  OpenMP over rows. */
+int oracle_u1_apply_rows(uint32_t n, uint32_t k, uint64_t count, const uint64_t *xw, const uint64_t *zw,
+                         const double *coef, const double *state, uint64_t nrows, const uint64_t *rows,
+                         double *out, int threads) {
+    uint64_t dim;
+    int st = oracle_u1_dimension(n, k, &dim);
+    if (st) return st;
+    u1terms t;
+    build_terms(n, count, xw, zw, coef, &t);
+    const uint32_t W = wcount(n);
+    const int complement = k > n - k;
+    int bad = 0;
+#pragma omp parallel num_threads(threads > 0 ? threads : 1)
+    {
+        uint64_t *dst = calloc(W + 1, sizeof(uint64_t)), *src = calloc(W + 1, sizeof(uint64_t));
+#pragma omp for schedule(static)
+        for (uint64_t r = 0; r < nrows; ++r) {
+            double yr = 0.0, yi = 0.0;
+            if (rows[r] >= dim || oracle_u1_unrank(n, k, rows[r], dst)) {
+                bad = 1;
+                continue;
+            }
+            for (uint64_t g = 0; g < t.ngroups; ++g) {
+                uint64_t weight = 0;
+                for (uint32_t w = 0; w < W; ++w) {
+                    src[w] = dst[w] ^ t.gx[g * W + w];
+                    weight += (uint64_t)__builtin_popcountll(src[w]);
+                }
+                if (weight != k) continue;
+                double vr = 0.0, vi = 0.0;
+                for (uint64_t i = t.gstart[g]; i < t.gstart[g + 1]; ++i) {
+                    if (z_parity(src, t.tz + i * W, W, complement, n)) {
+                        vr -= t.tw[i].re;
+                        vi -= t.tw[i].im;
+                    } else {
+                        vr += t.tw[i].re;
+                        vi += t.tw[i].im;
+                    }
+                }
+                if (vr == 0.0 && vi == 0.0) continue;
+                uint64_t s;
+                oracle_u1_rank(n, k, src, &s);
+                const double xr = state[2 * s], xi = state[2 * s + 1];
+                yr += vr * xr - vi * xi;
+                yi += vr * xi + vi * xr;
+            }
+            out[2 * r] = yr;
+            out[2 * r + 1] = yi;
+        }
+        free(dst);
+        free(src);
+    }
+    free_terms(&t);
+    return bad ? 13 : 0;
+}

@@ -244,33 +244,42 @@ struct U1Dev {
 // exchange; Jordan-Wigner hopping with one Z string), the group's value is
 // (-1)^{popcount(z_out & b)} * C with C summed once at plan build, in the
 // canonical term order from 0 as the reference sums it -- negating a sum term
-// by term negates it exactly, so the value is bit-identical.  Other groups
-// run the term loop.
+// by term negates it exactly, so the value is bit-identical.  A constant group
+// with C == 0 never contributes and is dropped.  The groups are laid out in
+// three segments -- constant without z_out (A), constant with z_out (B),
+// general (C, the term loop) -- each padded to a multiple of kU1Unroll with
+// groups that are never live (x = 0, half = 1).
 //
 // Fast ranks (n <= 32): rank(s) = H[top] + M[popcount(top)][mid] + L[low]
 // (three levels) or H[s >> L] + L[s & (2^L - 1)] (two levels, no middle):
 // H counts the sector states with a smaller top part, M those with the same
 // top part and a smaller middle part, L ranks the low bits among words of
 // their own weight.
-constexpr uint32_t kGroupConst = 1u << 31;  // ainfo: value is +-C
-constexpr uint32_t kGroupZout = 1u << 30;   // ainfo: sign by popcount(z_out & b)
-constexpr uint32_t kGroupHalf = 0xffffu;    // ainfo: popcount(x) / 2
+constexpr int kU1Unroll = 4;
+
+template <typename ST> struct GRec;
+template <> struct GRec<uint32_t> {
+    uint32_t x, half;
+};
+template <> struct GRec<uint64_t> {
+    uint64_t x;
+    uint32_t half, pad;
+};
 
 struct U1Apply {
     const uint32_t *ftab;  // fast rank tables (rk 2 or 3), else null
     uint32_t rk, rL, rM, lmask, mmask, h_off, m_off, l_off;
     size_t ftab_bytes;
-    const void *ax;        // ST[ga]: x masks
-    const uint32_t *ainfo; // [ga]: half | kGroupConst | kGroupZout
-    const void *azo;       // ST[ga]: z_out of constant groups
-    const double2 *ac;     // [ga]: C of constant groups
-    const float2 *acf;     // [ga]: C rounded to FP32
-    const uint32_t *at;    // [ga + 1]: term offsets (empty for constant groups)
+    const void *grec;      // GRec<ST>[na + nb + nc]: x mask and popcount(x) / 2
+    const double2 *ac;     // [na + nb]: C of the constant groups
+    const float2 *acf;     // [na + nb]: C rounded to FP32
+    const void *azo;       // ST[nb]: z_out of segment B
+    const uint32_t *at;    // [nc + 1]: term offsets of segment C
     const void *az;        // ST[ta]: term z masks
     const double2 *aw;     // [ta]
     const float2 *awf;     // [ta]
     const double2 *diag;   // [dim] or null when there is no x == 0 group
-    uint32_t ga, ta;
+    uint32_t na, nb, nc, ta;
 };
 
 template <typename R> struct Cplx;
@@ -310,19 +319,19 @@ __device__ __forceinline__ uint64_t rank_state(uint64_t s, const IT *__restrict_
 __host__ __device__ inline size_t al16(size_t v) { return (v + 15) & ~size_t(15); }
 
 struct U1ApplySmem {
-    size_t tab, ax, ai, azo, ac, at, az, aw, total;
+    size_t tab, grec, ac, azo, at, az, aw, total;
 };
 
-__host__ __device__ inline U1ApplySmem u1_apply_layout(size_t tab_bytes, uint32_t G, uint32_t T, size_t sbytes,
-                                                       size_t wbytes) {
+__host__ __device__ inline U1ApplySmem u1_apply_layout(size_t tab_bytes, uint32_t na, uint32_t nb, uint32_t nc,
+                                                       uint32_t T, size_t sbytes, size_t wbytes) {
+    const size_t rec = 2 * sbytes;  // GRec<ST>
     U1ApplySmem s;
     s.tab = 0;
-    s.ax = al16(tab_bytes);
-    s.ai = s.ax + al16(sbytes * G);
-    s.azo = s.ai + al16(4ull * G);
-    s.ac = s.azo + al16(sbytes * G);
-    s.at = s.ac + al16(wbytes * G);
-    s.az = s.at + al16(4ull * (G + 1));
+    s.grec = al16(tab_bytes);
+    s.ac = s.grec + al16(rec * (na + nb + nc));
+    s.azo = s.ac + al16(wbytes * (na + nb));
+    s.at = s.azo + al16(sbytes * nb);
+    s.az = s.at + al16(4ull * (nc + 1));
     s.aw = s.az + al16(sbytes * T);
     s.total = s.aw + al16(wbytes * T);
     return s;
@@ -365,53 +374,69 @@ __device__ __forceinline__ uint64_t rank_any(ST s, const IT *__restrict__ tab, c
     }
 }
 
+template <typename R, typename C>
+__device__ __forceinline__ void cmac(R &ar, R &ai, R &cr, R &ci, R vr, R vi, const C &xv) {
+    const R pr = vr * xv.x - vi * xv.y;
+    const R pi = vr * xv.y + vi * xv.x;
+    if (sizeof(R) == 8) {
+        ar += pr;
+        ai += pi;
+    } else {  // Kahan-compensated FP32 sum
+        const R yr = pr - cr, yi = pi - ci;
+        const R tr = ar + yr, ti = ai + yi;
+        cr = (tr - ar) - yr;
+        ci = (ti - ai) - yi;
+        ar = tr;
+        ai = ti;
+    }
+}
+
 // y = H_sector x.  One output row per thread, grid-stride over rows.  Row i
-// starts from diag[i] * x[i]; the other groups run in blocks of U: every
-// group of a block is tested (popcount(b & x) == |x| / 2), valued and ranked,
-// then the U gathers are issued back to back and accumulated in group order.
-// A skipped group (source outside the sector, or a value of exactly zero)
-// loads the thread's own row, which is always valid, and is not added.
+// starts from diag[i] * x[i]; then the three group segments.  A group is live
+// for row b when its source b ^ x lies in the sector (popcount(b & x) ==
+// |x| / 2).  Each block of kU1Unroll groups is tested and ranked first, its
+// gathers are issued back to back, then the live ones are accumulated.  A
+// group that is not live loads the thread's own row, which is always valid,
+// and is not added; neither is a general group whose value is exactly zero.
 template <typename R, typename ST, typename IT, int RK, bool SM, bool DIAG>
 __global__ void __launch_bounds__(kU1Threads) k_u1_apply(U1Dev p, U1Apply a, size_t tab_bytes,
                                                          const typename Cplx<R>::T *__restrict__ x,
                                                          typename Cplx<R>::T *__restrict__ y) {
     using C = typename Cplx<R>::T;
-    constexpr int U = 4;
+    using G = GRec<ST>;
+    constexpr int U = kU1Unroll;
     extern __shared__ __align__(16) unsigned char sm[];
     const IT *tab;
-    const ST *ax;
-    const uint32_t *ai;
-    const ST *azo;
+    const G *grec;
     const C *ac;
+    const ST *azo;
     const uint32_t *at;
     const ST *az;
     const C *aw;
     const void *tab_src = RK ? static_cast<const void *>(a.ftab) : p.tab;
+    const uint32_t nab = a.na + a.nb, nall = nab + a.nc;
     if (SM) {
-        const U1ApplySmem L = u1_apply_layout(tab_bytes, a.ga, a.ta, sizeof(ST), sizeof(C));
+        const U1ApplySmem L = u1_apply_layout(tab_bytes, a.na, a.nb, a.nc, a.ta, sizeof(ST), sizeof(C));
         copy16(sm + L.tab, tab_src, tab_bytes);
-        copy16(sm + L.ax, a.ax, sizeof(ST) * a.ga);
-        copy16(sm + L.ai, a.ainfo, 4ull * a.ga);
-        copy16(sm + L.azo, a.azo, sizeof(ST) * a.ga);
-        copy16(sm + L.ac, ApplyW<R>::consts(a), sizeof(C) * a.ga);
-        copy16(sm + L.at, a.at, 4ull * (a.ga + 1));
+        copy16(sm + L.grec, a.grec, sizeof(G) * nall);
+        copy16(sm + L.ac, ApplyW<R>::consts(a), sizeof(C) * nab);
+        copy16(sm + L.azo, a.azo, sizeof(ST) * a.nb);
+        copy16(sm + L.at, a.at, 4ull * (a.nc + 1));
         copy16(sm + L.az, a.az, sizeof(ST) * a.ta);
         copy16(sm + L.aw, ApplyW<R>::terms(a), sizeof(C) * a.ta);
         __syncthreads();
         tab = reinterpret_cast<const IT *>(sm + L.tab);
-        ax = reinterpret_cast<const ST *>(sm + L.ax);
-        ai = reinterpret_cast<const uint32_t *>(sm + L.ai);
-        azo = reinterpret_cast<const ST *>(sm + L.azo);
+        grec = reinterpret_cast<const G *>(sm + L.grec);
         ac = reinterpret_cast<const C *>(sm + L.ac);
+        azo = reinterpret_cast<const ST *>(sm + L.azo);
         at = reinterpret_cast<const uint32_t *>(sm + L.at);
         az = reinterpret_cast<const ST *>(sm + L.az);
         aw = reinterpret_cast<const C *>(sm + L.aw);
     } else {
         tab = static_cast<const IT *>(tab_src);
-        ax = static_cast<const ST *>(a.ax);
-        ai = a.ainfo;
-        azo = static_cast<const ST *>(a.azo);
+        grec = static_cast<const G *>(a.grec);
         ac = ApplyW<R>::consts(a);
+        azo = static_cast<const ST *>(a.azo);
         at = a.at;
         az = static_cast<const ST *>(a.az);
         aw = ApplyW<R>::terms(a);
@@ -420,80 +445,79 @@ __global__ void __launch_bounds__(kU1Threads) k_u1_apply(U1Dev p, U1Apply a, siz
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.dim; i += stride) {
         const ST b = basis[i];
-        R ar = 0, ai_ = 0, cr = 0, ci = 0;  // cr, ci: Kahan compensation (FP32 only)
+        R ar = 0, ai = 0, cr = 0, ci = 0;
         if (DIAG) {
             const double2 d = a.diag[i];
-            const C xv = x[i];
             const R dr = static_cast<R>(d.x), di = static_cast<R>(d.y);
             if (dr != R(0) || di != R(0)) {
+                const C xv = x[i];
                 ar = dr * xv.x - di * xv.y;
-                ai_ = dr * xv.y + di * xv.x;
+                ai = dr * xv.y + di * xv.x;
             }
         }
-        for (uint32_t g0 = 0; g0 < a.ga; g0 += U) {
+        // segments A and B: constant values
+        for (uint32_t g0 = 0; g0 < nab; g0 += U) {
+            bool live[U];
             uint64_t j[U];
-            R vr[U], vi[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const uint32_t g = g0 + u;
-                vr[u] = 0;
-                vi[u] = 0;
-                j[u] = i;
-                if (g >= a.ga) continue;
-                const ST xm = ax[g];
-                const uint32_t info = ai[g];
-                if (popc_t<ST>(b & xm) != (info & kGroupHalf)) continue;
-                const ST s = b ^ xm;
-                R wr = 0, wi = 0;
-                if (info & kGroupConst) {
-                    const C c = ac[g];
-                    wr = c.x;
-                    wi = c.y;
-                    if ((info & kGroupZout) && (popc_t<ST>(azo[g] & b) & 1u)) {
-                        wr = -wr;
-                        wi = -wi;
-                    }
-                } else {
-                    const uint32_t te = at[g + 1];
-                    for (uint32_t t = at[g]; t < te; ++t) {
-                        const C w = aw[t];
-                        if (popc_t<ST>(az[t] & s) & 1u) {
-                            wr -= w.x;
-                            wi -= w.y;
-                        } else {
-                            wr += w.x;
-                            wi += w.y;
-                        }
-                    }
-                }
-                vr[u] = wr;
-                vi[u] = wi;
-                if (wr != R(0) || wi != R(0)) j[u] = rank_any<RK, ST, IT>(s, tab, p, a);
+                const G r = grec[g0 + u];
+                live[u] = popc_t<ST>(b & r.x) == r.half;
+                j[u] = live[u] ? rank_any<RK, ST, IT>(b ^ r.x, tab, p, a) : i;
             }
             C xv[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) xv[u] = x[j[u]];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (vr[u] == R(0) && vi[u] == R(0)) continue;
-                const R pr = vr[u] * xv[u].x - vi[u] * xv[u].y;
-                const R pi = vr[u] * xv[u].y + vi[u] * xv[u].x;
-                if (sizeof(R) == 8) {
-                    ar += pr;
-                    ai_ += pi;
-                } else {
-                    const R yr = pr - cr, yi = pi - ci;
-                    const R tr = ar + yr, ti = ai_ + yi;
-                    cr = (tr - ar) - yr;
-                    ci = (ti - ai_) - yi;
-                    ar = tr;
-                    ai_ = ti;
+                if (!live[u]) continue;
+                const C c = ac[g0 + u];
+                R vr = c.x, vi = c.y;
+                if (g0 >= a.na && (popc_t<ST>(azo[g0 + u - a.na] & b) & 1u)) {
+                    vr = -vr;
+                    vi = -vi;
                 }
+                cmac<R, C>(ar, ai, cr, ci, vr, vi, xv[u]);
             }
+        }
+        // segment C: general groups, term by term
+        for (uint32_t g0 = nab; g0 < nall; g0 += U) {
+            bool live[U];
+            uint64_t j[U];
+            R vr[U], vi[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const G r = grec[g0 + u];
+                vr[u] = 0;
+                vi[u] = 0;
+                j[u] = i;
+                live[u] = popc_t<ST>(b & r.x) == r.half;
+                if (!live[u]) continue;
+                const ST s = b ^ r.x;
+                const uint32_t te = at[g0 + u - nab + 1];
+                for (uint32_t t = at[g0 + u - nab]; t < te; ++t) {
+                    const C w = aw[t];
+                    if (popc_t<ST>(az[t] & s) & 1u) {
+                        vr[u] -= w.x;
+                        vi[u] -= w.y;
+                    } else {
+                        vr[u] += w.x;
+                        vi[u] += w.y;
+                    }
+                }
+                live[u] = vr[u] != R(0) || vi[u] != R(0);
+                if (live[u]) j[u] = rank_any<RK, ST, IT>(s, tab, p, a);
+            }
+            C xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = x[j[u]];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (live[u]) cmac<R, C>(ar, ai, cr, ci, vr[u], vi[u], xv[u]);
         }
         C out;
         out.x = ar;
-        out.y = ai_;
+        out.y = ai;
         y[i] = out;
     }
 }
@@ -821,22 +845,15 @@ int upload(tcp_u1_plan *p) {
     if (p->index32) tab32.assign(tab.begin(), tab.end());
     std::vector<float> twf(2 * static_cast<size_t>(T));
     for (size_t i = 0; i < twf.size(); ++i) twf[i] = static_cast<float>(t.tw[i]);
-    // apply view: groups with x != 0 and an even number of flips
+    // apply view: groups with x != 0 and an even number of flips, in three
+    // segments (constant, constant with z_out, general); see U1Apply
     const size_t ssz = p->basis32 ? 4 : 8;
-    std::vector<unsigned char> ax, azo, az;
-    std::vector<uint32_t> ainfo, at(1, 0);
-    std::vector<double> ac, aw;
-    std::vector<float> acf, awf;
-    auto put = [&](std::vector<unsigned char> &v, uint64_t m) {
-        const size_t o = v.size();
-        v.resize(o + ssz);
-        if (ssz == 4) {
-            const uint32_t m32 = static_cast<uint32_t>(m);
-            std::memcpy(v.data() + o, &m32, 4);
-        } else {
-            std::memcpy(v.data() + o, &m, 8);
-        }
+    struct SegGroup {
+        uint64_t x, zout;
+        uint32_t half, tb, te;
+        double cr, ci;
     };
+    std::vector<SegGroup> segA, segB, segC;
     for (uint32_t g = 0; g < G; ++g) {
         const uint64_t x = t.gx[g];
         const uint32_t w = static_cast<uint32_t>(__builtin_popcountll(x));
@@ -848,41 +865,75 @@ int upload(tcp_u1_plan *p) {
             const uint64_t zin = t.tz[q] & x;
             constant = (zin == 0 || zin == x) && (t.tz[q] & ~x) == zout;
         }
-        put(ax, x);
-        put(azo, zout);
-        uint32_t info = w / 2;
-        double cr = 0.0, ci = 0.0;
-        if (constant) {
-            // the group value where popcount(z_out & b) is even, summed from 0
-            // in canonical term order as aggregate_source sums it
-            for (uint32_t q = tb; q < te; ++q) {
-                const bool neg = ((t.tz[q] & x) == x) && ((w / 2) & 1);
-                if (neg) {
-                    cr -= t.tw[2 * q];
-                    ci -= t.tw[2 * q + 1];
-                } else {
-                    cr += t.tw[2 * q];
-                    ci += t.tw[2 * q + 1];
-                }
-            }
-            info |= kGroupConst | (zout ? kGroupZout : 0u);
-        } else {
-            for (uint32_t q = tb; q < te; ++q) {
-                put(az, t.tz[q]);
-                aw.push_back(t.tw[2 * q]);
-                aw.push_back(t.tw[2 * q + 1]);
-                awf.push_back(twf[2 * q]);
-                awf.push_back(twf[2 * q + 1]);
+        SegGroup sg{x, zout, w / 2, tb, te, 0.0, 0.0};
+        if (!constant) {
+            segC.push_back(sg);
+            continue;
+        }
+        // the value where popcount(z_out & b) is even, summed from 0 in
+        // canonical term order as aggregate_source sums it
+        for (uint32_t q = tb; q < te; ++q) {
+            if (((t.tz[q] & x) == x) && ((w / 2) & 1)) {
+                sg.cr -= t.tw[2 * q];
+                sg.ci -= t.tw[2 * q + 1];
+            } else {
+                sg.cr += t.tw[2 * q];
+                sg.ci += t.tw[2 * q + 1];
             }
         }
-        ainfo.push_back(info);
-        ac.push_back(cr);
-        ac.push_back(ci);
-        acf.push_back(static_cast<float>(cr));
-        acf.push_back(static_cast<float>(ci));
+        if (sg.cr == 0.0 && sg.ci == 0.0) continue;  // never contributes
+        (zout ? segB : segA).push_back(sg);
+    }
+    auto pad = [](std::vector<SegGroup> &v) {
+        while (v.size() % kU1Unroll) v.push_back(SegGroup{0, 0, 1, 0, 0, 0.0, 0.0});  // never live
+    };
+    pad(segA);
+    pad(segB);
+    pad(segC);
+    std::vector<unsigned char> grec, azo, az;
+    std::vector<double> ac, aw;
+    std::vector<float> acf, awf;
+    std::vector<uint32_t> at(1, 0);
+    auto put = [&](std::vector<unsigned char> &v, uint64_t m) {
+        const size_t o = v.size();
+        v.resize(o + ssz);
+        if (ssz == 4) {
+            const uint32_t m32 = static_cast<uint32_t>(m);
+            std::memcpy(v.data() + o, &m32, 4);
+        } else {
+            std::memcpy(v.data() + o, &m, 8);
+        }
+    };
+    auto put_rec = [&](const SegGroup &sg) {
+        put(grec, sg.x);
+        const uint32_t half_pad[2] = {sg.half, 0};
+        const size_t o = grec.size();
+        grec.resize(o + ssz);  // half (and padding for 64-bit records)
+        std::memcpy(grec.data() + o, half_pad, ssz);
+    };
+    for (auto *seg : {&segA, &segB}) {
+        for (const SegGroup &sg : *seg) {
+            put_rec(sg);
+            ac.push_back(sg.cr);
+            ac.push_back(sg.ci);
+            acf.push_back(static_cast<float>(sg.cr));
+            acf.push_back(static_cast<float>(sg.ci));
+        }
+    }
+    for (const SegGroup &sg : segB) put(azo, sg.zout);
+    for (const SegGroup &sg : segC) {
+        put_rec(sg);
+        for (uint32_t q = sg.tb; q < sg.te; ++q) {
+            put(az, t.tz[q]);
+            aw.push_back(t.tw[2 * q]);
+            aw.push_back(t.tw[2 * q + 1]);
+            awf.push_back(twf[2 * q]);
+            awf.push_back(twf[2 * q + 1]);
+        }
         at.push_back(static_cast<uint32_t>(aw.size() / 2));
     }
-    const uint32_t GA = static_cast<uint32_t>(ainfo.size()), TA = at.back();
+    const uint32_t NA = static_cast<uint32_t>(segA.size()), NB = static_cast<uint32_t>(segB.size()),
+                   NC = static_cast<uint32_t>(segC.size()), TA = at.back();
     const bool has_diag = t.gzero >= 0;
     // fast rank tables (n <= 32): two levels up to 24 qubits, else three
     std::vector<uint32_t> ftab;
@@ -953,12 +1004,12 @@ int upload(tcp_u1_plan *p) {
         {t.tw.data(), 16ull * T, 0},
         {twf.data(), 8ull * T, 0},
         {nullptr, bsz * p->dim, 0},  // basis, generated on the device
-        {ax.data(), ax.size(), 0},
-        {ainfo.data(), 4ull * GA, 0},
+        {grec.data(), grec.size(), 0},
+        {nullptr, 0, 0},
         {azo.data(), azo.size(), 0},
         {ac.data(), 8ull * ac.size(), 0},
         {acf.data(), 4ull * acf.size(), 0},
-        {at.data(), 4ull * (GA + 1), 0},
+        {at.data(), 4ull * at.size(), 0},
         {az.data(), az.size(), 0},
         {aw.data(), 8ull * aw.size(), 0},
         {awf.data(), 4ull * awf.size(), 0},
@@ -1008,8 +1059,7 @@ int upload(tcp_u1_plan *p) {
     d.nterms = T;
     U1Apply &ap = p->app;
     ap = fast;
-    ap.ax = base + pieces[8].off;
-    ap.ainfo = reinterpret_cast<const uint32_t *>(base + pieces[9].off);
+    ap.grec = base + pieces[8].off;
     ap.azo = base + pieces[10].off;
     ap.ac = reinterpret_cast<const double2 *>(base + pieces[11].off);
     ap.acf = reinterpret_cast<const float2 *>(base + pieces[12].off);
@@ -1019,7 +1069,9 @@ int upload(tcp_u1_plan *p) {
     ap.awf = reinterpret_cast<const float2 *>(base + pieces[16].off);
     ap.diag = has_diag ? reinterpret_cast<const double2 *>(base + pieces[17].off) : nullptr;
     ap.ftab = p->basis32 ? reinterpret_cast<const uint32_t *>(base + pieces[18].off) : nullptr;
-    ap.ga = GA;
+    ap.na = NA;
+    ap.nb = NB;
+    ap.nc = NC;
     ap.ta = TA;
     // basis generation
     const uint32_t rows_per_thread = 64;
@@ -1043,8 +1095,8 @@ int upload(tcp_u1_plan *p) {
     }
     // shared-memory staging of the apply view
     const size_t apply_tab = p->basis32 ? ap.ftab_bytes : p->tab_bytes;
-    p->smem_c128 = u1_apply_layout(apply_tab, GA, TA, ssz, 16).total;
-    p->smem_c64 = u1_apply_layout(apply_tab, GA, TA, ssz, 8).total;
+    p->smem_c128 = u1_apply_layout(apply_tab, NA, NB, NC, TA, ssz, 16).total;
+    p->smem_c64 = u1_apply_layout(apply_tab, NA, NB, NC, TA, ssz, 8).total;
     p->smem = p->smem_c128 <= kU1SmemMax;
     return TCP_OK;
 }
