@@ -462,9 +462,9 @@ def run_chemistry(args: argparse.Namespace) -> None:
 
 
 def run_sector(args: argparse.Namespace) -> None:
-    """Restricted MVP in the half-filling U(1) sector of the periodic 4x7
-    J1-J2 model (J1 = 1, J2 = 0.5; n = 28, k = 14, dimension C(28, 14) =
-    40,116,600).  A step is one y = H x over the whole restricted state.
+    """Restricted MVP in the half-filling U(1) sector of the periodic J1-J2
+    model (J1 = 1, J2 = 0.5) on ``--lattice`` (default 4x7: n = 28, k = 14,
+    dimension C(28, 14) = 40,116,600).  A step is one y = H x over the whole restricted state.
     Metric: restricted amplitude-terms/s = T_canonical * dimension / step
     time.  ``e2e`` runs the host C-ABI apply (pinned buffers, H2D + kernel +
     D2H); ``cpu_baseline`` pulls a bounded sample of rows with the oracle."""
@@ -473,7 +473,7 @@ def run_sector(args: argparse.Namespace) -> None:
     from tencirpauli_b200 import PauliOperator, U1Sector, workloads
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    lx, ly = 4, 7
+    lx, ly = (int(v) for v in args.lattice.lower().split("x"))
     n, k = lx * ly, (lx * ly) // 2
     op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(lx, ly, 1.0, 0.5))
     t0 = time.perf_counter()
@@ -556,9 +556,9 @@ def run_sector(args: argparse.Namespace) -> None:
         "vs_baseline": None,
         "dtype": "f64" if args.dtype == "c128" else "f32",
         "data": "synthetic",
-        "config": {"workload": "periodic 4x7 J1-J2 (J1=1, J2=0.5), half-filling U(1) sector", "nqubits": n,
+        "config": {"workload": f"periodic {lx}x{ly} J1-J2 (J1=1, J2=0.5), half-filling U(1) sector", "nqubits": n,
                    "particle_number": k, "dimension": dim, "terms": T, "groups": native.group_count,
-                   "l2": "restricted state 642 MB > L2; no flush needed"},
+                   "l2": f"restricted state {dim * 16 / 1e6:.0f} MB" + ("; > L2, no flush needed" if dim * 16 > 126e6 else "; fits in L2")},
         "roofline": {"bound": "issue (integer/FP64 instruction rate; HBM bytes shown for reference)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "kernel": "k_u1_apply", "bytes_per_launch": b_alg,
@@ -583,6 +583,7 @@ def main() -> None:
     parser.add_argument("--workload", choices=["random28", "batched", "davidson", "chemistry", "sector"],
                         default="random28")
     parser.add_argument("--batch-count", type=int, default=64)
+    parser.add_argument("--lattice", default="4x7", help="sector workload: periodic J1-J2 lattice LXxLY")
     parser.add_argument("--batch-rhs", type=int, default=8)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=10)
@@ -708,6 +709,17 @@ def main() -> None:
         achieved = b_alg / (kern_ms / 1000.0) / 1e9
         kernel_name = "k_tiled<3,double>" if args.dtype == "c128" else "k_tiled<3,float>"
         traffic = _profile_traffic(kernel_name)
+        # The binding ceiling is the FMA pipe: F_alg = 2^n (2T + 8G) real flops
+        # (the +-w_k sums into D_m once per amplitude, one complex multiply-add
+        # per group), against this GPU's own FMA rate.
+        from tencirpauli_b200 import _native as native_mod
+
+        fma_rate, _ = native_mod.probe_fma_rate("complex128" if args.dtype == "c128" else "complex64")
+        G = plan.group_count
+        f_alg = dim * (2 * T + 8 * G)
+        f_ach = f_alg / (kern_ms / 1000.0)
+        smem_bytes = dim * G * elem  # one operand per (row, group) from shared memory
+        smem_peak = 128.0 * torch.cuda.get_device_properties(0).multi_processor_count * 1.965e9
         line = {
             "metric": METRIC,
             "value": value,
@@ -723,16 +735,31 @@ def main() -> None:
             "data": "synthetic",
             "config": workload_config(args, op),
             "roofline": {
-                "bound": "hbm",
-                "achieved": achieved,
-                "peak": peaks["hbm_gbs"],
-                "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"],
+                "bound": "fp64" if args.dtype == "c128" else "fp32",
+                "achieved": f_ach / 1e12,
+                "peak": fma_rate / 1e12,
+                "unit": "TFLOP/s",
+                "frac": f_ach / fma_rate,
                 "traffic": traffic,
-                "peak_source": peaks["source"],
+                "peak_source": "tcp_probe_fma_rate: FMA chains on every SM of this GPU, best of 5",
                 "kernel": kernel_name,
-                "bytes_per_launch": b_alg,
+                "flops_per_launch": f_alg,
                 "kernel_ms": kern_ms,
+                "hbm": {
+                    "achieved": achieved,
+                    "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"],
+                    "bytes_per_launch": b_alg,
+                    "peak_source": peaks["source"],
+                    "traffic_gbs": (traffic / (kern_ms / 1000.0) / 1e9) if traffic else None,
+                },
+                "smem_operands": {
+                    "bytes_per_launch": smem_bytes,
+                    "achieved_tbs": smem_bytes / (kern_ms / 1000.0) / 1e12,
+                    "nominal_peak_tbs": smem_peak / 1e12,
+                    "frac": smem_bytes / (kern_ms / 1000.0) / smem_peak,
+                },
             },
             "e2e": {
                 "value": e2e_value,

@@ -106,6 +106,10 @@ SECTOR_SYMBOLS = (
 )
 
 
+# Every symbol include/tcp_probe.h declares.
+PROBE_SYMBOLS = ("tcp_probe_fma_rate",)
+
+
 class TcpU1PlanInfo(ctypes.Structure):
     _fields_ = [
         ("nqubits", ctypes.c_uint32),
@@ -220,6 +224,8 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_u1_plan_device_status.argtypes = [vp]
         for name in SECTOR_SYMBOLS:
             getattr(lib, name).restype = i32
+        lib.tcp_probe_fma_rate.argtypes = [i32, u32, f64p, f64p]
+        lib.tcp_probe_fma_rate.restype = i32
         for name in SOLVER_SYMBOLS:
             if not name.endswith("_work_bytes"):
                 getattr(lib, name).restype = i32
@@ -793,3 +799,15 @@ class NativeU1Plan:
 
     def device_status(self) -> None:
         raise_for_status(self._lib.tcp_u1_plan_device_status(self._handle))
+
+
+def probe_fma_rate(dtype: str = "complex128", repeats: int = 5) -> Tuple[float, float]:
+    """(flop/s, best launch ms) of the device's FP64 (complex128) or FP32
+    (complex64) FMA pipe, measured by ``tcp_probe_fma_rate``."""
+    rate = np.zeros(1, np.float64)
+    ms = np.zeros(1, np.float64)
+    code = TCP_DTYPE_C128 if dtype in ("complex128", "c128") else TCP_DTYPE_C64
+    raise_for_status(
+        load_library().tcp_probe_fma_rate(code, repeats, _ptr(rate, ctypes.c_double), _ptr(ms, ctypes.c_double))
+    )
+    return float(rate[0]), float(ms[0])

@@ -34,6 +34,10 @@ def test_library_loads_and_exports_every_declared_symbol() -> None:
     assert set(solver) == set(_native.SOLVER_SYMBOLS)
     for name in solver:
         assert hasattr(lib, name), name
+    probe = _declared_functions("tcp_probe.h")
+    assert set(probe) == set(_native.PROBE_SYMBOLS)
+    for name in probe:
+        assert hasattr(lib, name), name
     sector = _declared_functions("tcp_sector.h")
     assert set(sector) == set(_native.SECTOR_SYMBOLS)
     for name in sector:
