@@ -84,9 +84,9 @@ __device__ __forceinline__ void apply_term(ulonglong2 rec, typename Cx<R>::T w, 
     }
 }
 
-// Terms of one x-mask group applied to the thread's E rows.  JH (the group's
-// inner-mask bits above the thread index) is a template parameter, so row j
-// reads the loaded source value jj = j ^ JH at a compile-time register index.
+// Terms of one x-mask group applied to the thread's E rows.  JH is a
+// compile-time row permutation between the loaded values and the rows; the
+// tiled kernel loads its values in row order already (JH = 0).
 // Term records come from the step block in shared memory; a term whose z mask
 // has no bit among the thread's row bits (pattern 0) has one sign for all E
 // rows, otherwise the sign of source jj is bit jj of the pattern.
@@ -100,29 +100,16 @@ __device__ __forceinline__ void apply_group(const unsigned char *__restrict__ tr
     }
 }
 
-// Dispatch a group on its inner-mask bits above the thread index.
-template <int LOGE, typename R>
-__device__ __forceinline__ void dispatch_group(uint32_t jh, const unsigned char *__restrict__ trm, uint32_t tb,
-                                               uint32_t te, uint32_t tid, uint64_t tile,
-                                               const typename Cx<R>::T (&xv)[1 << LOGE], Acc<R> (&acc)[1 << LOGE]) {
-    switch (jh) {
-    case 0: apply_group<0, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    case 1: apply_group<1, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    case 2: apply_group<2, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    case 3: apply_group<3, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    case 4: apply_group<4, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    case 5: apply_group<5, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    case 6: apply_group<6, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    default: apply_group<7, LOGE, R>(trm, tb, te, tid, tile, xv, acc); break;
-    }
-}
-
-// Source values of one group for the thread: xv[jj] = tile[(tid ^ m_lo) + jj * T].
+// Source values of one group for the thread, in row order: row j of the
+// thread (tile row tid + j * T) reads source tile row (tid ^ m_lo) +
+// (j ^ jh) * T, where m_lo and jh are the group's inner-mask bits at and
+// above the thread index.
 template <int LOGE, typename C>
 __device__ __forceinline__ void load_group(const C *__restrict__ xs, uint32_t tid, uint32_t m, C (&xv)[1 << LOGE]) {
     const C *src = xs + (tid ^ (m & (kThreads - 1)));
+    const uint32_t jh = m >> kLogThreads;
 #pragma unroll
-    for (int jj = 0; jj < (1 << LOGE); ++jj) xv[jj] = src[jj << kLogThreads];
+    for (int j = 0; j < (1 << LOGE); ++j) xv[j] = src[(static_cast<uint32_t>(j) ^ jh) << kLogThreads];
 }
 
 template <typename R> __device__ __forceinline__ const unsigned char *step_blocks(const DevSchedule &s);
@@ -200,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint4 gr = grp[g];
             C xv[E];
             load_group<LOGE>(xs, tid, gr.x, xv);
-            dispatch_group<LOGE, R>(gr.x >> kLogThreads, trm, gr.y, gr.z, tid, tile, xv, acc);
+            apply_group<0, LOGE, R>(trm, gr.y, gr.z, tid, tile, xv, acc);
             // FP32: fold the running group sum into the compensated row sum
             // every kCompensateGroups groups and at the end of the step.
             if (((g + 1) % kCompensateGroups) == 0u || g + 1 == ng) {

@@ -169,10 +169,15 @@ Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, 
                 const uint32_t kind = (t.w_im == 0.0) ? kKindReal : ((t.w_re == 0.0) ? kKindImag : kKindComplex);
                 const uint64_t zrec = static_cast<uint64_t>(zlo) | (static_cast<uint64_t>(pattern) << 32) |
                                       (static_cast<uint64_t>(kind) << 56);
-                // parity(zt & d) and parity(zlo & m_lo) are fixed for the term
-                // inside its step and group, so they are folded into the weight.
+                // parity(zt & d), parity(zlo & m_lo) and parity(zj & jh) are
+                // fixed for the term inside its step and group, so they are
+                // folded into the weight.  (The kernel loads row j's source
+                // j ^ jh into register j, so the remaining sign of row j is
+                // bit j of the pattern, parity(zj & j), XOR the thread's base.)
                 const uint32_t m_lo = g.m_in & ((1u << L) - 1u);
-                const bool flip = ((__builtin_popcountll(zt & cur_d) + __builtin_popcount(zlo & m_lo)) & 1) != 0;
+                const uint32_t jh = g.m_in >> L;
+                const bool flip = ((__builtin_popcountll(zt & cur_d) + __builtin_popcount(zlo & m_lo) +
+                                    __builtin_popcount(zj & jh)) & 1) != 0;
                 const double wr = flip ? -t.w_re : t.w_re, wi = flip ? -t.w_im : t.w_im;
                 put(s.blocks_c128, zrec);
                 put(s.blocks_c128, zt);
