@@ -480,3 +480,92 @@ int oracle_max_threads(void) {
     return 1;
 #endif
 }
+
+/* PauliOperator::dense_matrix (hamiltonian.rs:313-355): row-major dense
+ * matrix; every row walks the terms in canonical order and adds (or
+ * subtracts) the weighted phase at column row ^ x_mask, the sign taken on the
+ * column.  out: complex128[dim * dim], zeroed here. */
+int oracle_dense(uint32_t nqubits, uint64_t count, const uint64_t *x_mask, const uint64_t *z_mask,
+                 const double *weighted, double *out) {
+    const uint64_t dim = 1ull << nqubits;
+    memset(out, 0, sizeof(double) * 2 * dim * dim);
+    for (uint64_t row = 0; row < dim; ++row) {
+        double *o = out + 2 * row * dim;
+        for (uint64_t t = 0; t < count; ++t) {
+            const uint64_t column = row ^ x_mask[t];
+            if (parity64(z_mask[t] & column)) {
+                o[2 * column] -= weighted[2 * t];
+                o[2 * column + 1] -= weighted[2 * t + 1];
+            } else {
+                o[2 * column] += weighted[2 * t];
+                o[2 * column + 1] += weighted[2 * t + 1];
+            }
+        }
+    }
+    return 0;
+}
+
+typedef struct {
+    uint64_t column;
+    double re, im;
+} sparse_entry;
+
+static int entry_cmp(const void *a, const void *b) {
+    const sparse_entry *x = a, *y = b;
+    return x->column < y->column ? -1 : (x->column > y->column ? 1 : 0);
+}
+
+/* sparse_entries / fill_sparse_row (hamiltonian.rs:584-752): per row, one
+ * entry per x-mask group (groups ascending by mask) whose value -- the group's
+ * weighted phases summed from 0 in canonical order with the column's signs --
+ * is not exactly zero, sorted by column.  Call with capacity 0 for *nnz;
+ * indptr has dim + 1 entries. */
+int oracle_csr(uint32_t nqubits, uint64_t count, const uint64_t *x_mask, const uint64_t *z_mask,
+               const double *weighted, uint64_t *indptr, uint64_t *columns, double *values, uint64_t capacity,
+               uint64_t *nnz) {
+    const uint64_t dim = 1ull << nqubits;
+    uint64_t *order = malloc(sizeof(uint64_t) * (count + 1));
+    uint64_t *gstart = malloc(sizeof(uint64_t) * (count + 1));
+    const uint64_t groups = group_terms(count, x_mask, order, gstart);
+    sparse_entry *row_entries = malloc(sizeof(sparse_entry) * (groups + 1));
+    uint64_t total = 0;
+    indptr[0] = 0;
+    for (uint64_t row = 0; row < dim; ++row) {
+        uint64_t m = 0;
+        for (uint64_t gi = 0; gi < groups; ++gi) {
+            const uint64_t column = row ^ x_mask[order[gstart[gi]]];
+            double re = 0.0, im = 0.0;
+            for (uint64_t i = gstart[gi]; i < gstart[gi + 1]; ++i) {
+                const uint64_t t = order[i];
+                double cr = weighted[2 * t], ci = weighted[2 * t + 1];
+                if (parity64(z_mask[t] & column)) {
+                    cr = -cr;
+                    ci = -ci;
+                }
+                re = re + cr;
+                im = im + ci;
+            }
+            if (re != 0.0 || im != 0.0) {
+                row_entries[m].column = column;
+                row_entries[m].re = re;
+                row_entries[m].im = im;
+                ++m;
+            }
+        }
+        qsort(row_entries, m, sizeof(sparse_entry), entry_cmp);
+        if (capacity) {
+            for (uint64_t e = 0; e < m && total + e < capacity; ++e) {
+                columns[total + e] = row_entries[e].column;
+                values[2 * (total + e)] = row_entries[e].re;
+                values[2 * (total + e) + 1] = row_entries[e].im;
+            }
+        }
+        total += m;
+        indptr[row + 1] = total;
+    }
+    *nnz = total;
+    free(row_entries);
+    free(gstart);
+    free(order);
+    return 0;
+}

@@ -16,6 +16,8 @@ project ``crates/tencir-pauli-core/src``):
 * :func:`apply_xmask_diagonal` -- ``hamiltonian.rs:79-147,233-235`` (eager plan)
 * :func:`transition_count`   -- ``hamiltonian.rs:166-179``
 * :func:`apply_rows`         -- the TermDirect row loop on selected rows only
+* :func:`dense`              -- ``hamiltonian.rs:313-355`` (``dense_matrix``)
+* :func:`csr`                -- ``hamiltonian.rs:584-752`` (sparse rows, sorted columns)
 
 U(1) sector items (``oracle/u1_oracle.c``, paths in ``sector.rs``):
 
@@ -69,6 +71,10 @@ def _load() -> ctypes.CDLL:
         lib.oracle_packed_word_count.argtypes = [u32]
         lib.oracle_packed_word_count.restype = u32
         lib.oracle_max_threads.restype = i32
+        lib.oracle_dense.argtypes = [u32, u64, _u64p, _u64p, _f64p, _f64p]
+        lib.oracle_csr.argtypes = [u32, u64, _u64p, _u64p, _f64p, _u64p, _u64p, _f64p, u64, _u64p]
+        lib.oracle_dense.restype = i32
+        lib.oracle_csr.restype = i32
         lib.oracle_u1_dimension.argtypes = [u32, u32, _u64p]
         lib.oracle_u1_rank.argtypes = [u32, u32, _u64p, _u64p]
         lib.oracle_u1_unrank.argtypes = [u32, u32, u64, _u64p]
@@ -428,3 +434,44 @@ def u1_apply_rows(nqubits: int, particle_number: int, x_words: np.ndarray, z_wor
     if status:
         raise OracleError(status)
     return out[: len(r)]
+
+
+def dense(nqubits: int, x_mask: np.ndarray, z_mask: np.ndarray, weighted: np.ndarray) -> np.ndarray:
+    """Dense row-major matrix (``PauliOperator::dense_matrix``)."""
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    zm = np.ascontiguousarray(z_mask, dtype=np.uint64)
+    w = np.ascontiguousarray(weighted, dtype=np.complex128)
+    dim = 1 << nqubits
+    out = np.zeros((dim, dim), np.complex128)
+    status = _load().oracle_dense(nqubits, len(xm), _p(xm if len(xm) else np.zeros(1, np.uint64), _u64p),
+                                  _p(zm if len(zm) else np.zeros(1, np.uint64), _u64p),
+                                  _p((w if len(w) else np.zeros(1, np.complex128)).view(np.float64), _f64p),
+                                  _p(out.view(np.float64), _f64p))
+    if status:
+        raise OracleError(status)
+    return out
+
+
+def csr(nqubits: int, x_mask: np.ndarray, z_mask: np.ndarray, weighted: np.ndarray):
+    """(indptr, columns, values) of the sparse rows (``sparse_entries``)."""
+    xm = np.ascontiguousarray(x_mask, dtype=np.uint64)
+    zm = np.ascontiguousarray(z_mask, dtype=np.uint64)
+    w = np.ascontiguousarray(weighted, dtype=np.complex128)
+    if len(xm) == 0:
+        xm = np.zeros(1, np.uint64); zm = np.zeros(1, np.uint64); w = np.zeros(1, np.complex128)
+        count = 0
+    else:
+        count = len(xm)
+    dim = 1 << nqubits
+    indptr = np.zeros(dim + 1, np.uint64)
+    nnz = np.zeros(1, np.uint64)
+    lib = _load()
+    one_c, one_v = np.zeros(1, np.uint64), np.zeros(2, np.float64)
+    lib.oracle_csr(nqubits, count, _p(xm, _u64p), _p(zm, _u64p), _p(w.view(np.float64), _f64p), _p(indptr, _u64p),
+                   _p(one_c, _u64p), _p(one_v, _f64p), 0, _p(nnz, _u64p))
+    m = int(nnz[0])
+    cols = np.zeros(max(m, 1), np.uint64)
+    vals = np.zeros(max(m, 1), np.complex128)
+    lib.oracle_csr(nqubits, count, _p(xm, _u64p), _p(zm, _u64p), _p(w.view(np.float64), _f64p), _p(indptr, _u64p),
+                   _p(cols, _u64p), _p(vals.view(np.float64), _f64p), m, _p(nnz, _u64p))
+    return indptr, cols[:m], vals[:m]

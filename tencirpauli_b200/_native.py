@@ -106,6 +106,11 @@ SECTOR_SYMBOLS = (
 )
 
 
+# Every symbol include/tcp_matrix.h declares.
+MATRIX_SYMBOLS = ("tcp_mvp_dense", "tcp_mvp_sparse_count", "tcp_mvp_csr")
+TCP_MATRIX_COO = 0
+TCP_MATRIX_CSR = 1
+
 # Every symbol include/tcp_probe.h declares.
 PROBE_SYMBOLS = ("tcp_probe_fma_rate",)
 
@@ -223,6 +228,11 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_u1_csr.argtypes = [vp, u64p, u64p, f64p, u64, u64p]
         lib.tcp_u1_plan_device_status.argtypes = [vp]
         for name in SECTOR_SYMBOLS:
+            getattr(lib, name).restype = i32
+        lib.tcp_mvp_dense.argtypes = [vp, f64p, u64, u64]
+        lib.tcp_mvp_sparse_count.argtypes = [vp, i32, u64, u64p]
+        lib.tcp_mvp_csr.argtypes = [vp, i32, u64, u64p, u64p, f64p, u64, u64p]
+        for name in MATRIX_SYMBOLS:
             getattr(lib, name).restype = i32
         lib.tcp_probe_fma_rate.argtypes = [i32, u32, f64p, f64p]
         lib.tcp_probe_fma_rate.restype = i32
@@ -516,6 +526,37 @@ class NativeMvpPlan:
     def device_status(self) -> None:
         """Synchronise and raise if a kernel of this plan reported a device error."""
         raise_for_status(self._lib.tcp_mvp_plan_device_status(self._handle))
+
+    # -- materialisation (include/tcp_matrix.h) ------------------------------
+    def dense(self, max_bytes: int) -> np.ndarray:
+        """Row-major complex128 dense matrix (``pauli_dense_handle``)."""
+        dim = self.dimension
+        if dim * dim * 16 > min(int(max_bytes), U64_MAX):
+            raise MemoryError(f"requested {dim * dim * 16} bytes exceeds memory limit {max_bytes}")
+        out = np.zeros((dim, dim), np.complex128)
+        raise_for_status(
+            self._lib.tcp_mvp_dense(self._handle, _ptr(out.view(np.float64), ctypes.c_double), dim * dim,
+                                    min(int(max_bytes), U64_MAX))
+        )
+        return out
+
+    def sparse(self, target: str, max_bytes: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(indptr, columns, values) with the budget of ``target`` ("coo" or "csr")."""
+        code = TCP_MATRIX_COO if target == "coo" else TCP_MATRIX_CSR
+        limit = min(int(max_bytes), U64_MAX)
+        nnz = np.zeros(1, np.uint64)
+        raise_for_status(self._lib.tcp_mvp_sparse_count(self._handle, code, limit, _ptr(nnz, ctypes.c_uint64)))
+        m = int(nnz[0])
+        indptr = np.zeros(self.dimension + 1, np.uint64)
+        cols = np.zeros(max(m, 1), np.uint64)
+        vals = np.zeros(max(m, 1), np.complex128)
+        raise_for_status(
+            self._lib.tcp_mvp_csr(self._handle, code, limit, _ptr(indptr, ctypes.c_uint64), _ptr(cols, ctypes.c_uint64),
+                                  _ptr(vals.view(np.float64), ctypes.c_double), cols.shape[0],
+                                  _ptr(nnz, ctypes.c_uint64))
+        )
+        m = int(nnz[0])
+        return indptr, cols[:m], vals[:m]
 
 
 # ----------------------------------------------------------------------------

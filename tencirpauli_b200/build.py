@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIBPATH = os.path.join(LIBDIR, "libtcpmvp.so")
-SOURCES = ["tcp_plan.cpp", "tcp_mvp.cu", "tcp_batched.cu", "tcp_solver.cu", "tcp_sector.cu", "tcp_probe.cu"]
+SOURCES = ["tcp_plan.cpp", "tcp_mvp.cu", "tcp_batched.cu", "tcp_solver.cu", "tcp_sector.cu", "tcp_probe.cu", "tcp_matrix.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -241,14 +241,50 @@ class PauliOperator:
         storage: Literal["lazy", "eager"] = "lazy",
         max_bytes: Optional[int] = DEFAULT_MAX_BYTES,
     ) -> Any:
-        """Compile a named target.  The B200 build implements ``"native_mvp"``."""
+        """Compile one named target (``pauli.py:1047-1072`` of the reference):
+        ``dense``, ``coo``, ``csr``, ``native_mvp`` or ``backend_mvp``."""
+        if target == "dense":
+            return self.dense(max_bytes=max_bytes)
+        if target == "coo":
+            return self.coo(max_bytes=max_bytes)
+        if target == "csr":
+            return self.csr(max_bytes=max_bytes)
         if target == "native_mvp":
             return self.native_mvp_plan(storage=storage, max_bytes=max_bytes)
         if target == "backend_mvp":
             from .backend import BackendMVPPlan
 
             return BackendMVPPlan.from_operator(self, max_bytes=max_bytes)
-        raise ValueError("target must be one of 'native_mvp' or 'backend_mvp'")
+        raise ValueError("target must be one of 'dense', 'coo', 'csr', 'native_mvp', or 'backend_mvp'")
+
+    # -- materialisation (``pauli.py:866-930`` of the reference) ----------------
+    def _matrix_plan(self) -> Any:
+        return _native.NativeMvpPlan(self.nqubits, self._x_words, self._z_words, self._coefficients, storage="lazy")
+
+    def dense(self, *, max_bytes: Optional[int] = DEFAULT_MAX_BYTES) -> np.ndarray:
+        """Bounded complex128 dense matrix, qubit 0 the most significant bit."""
+        validate_max_bytes(max_bytes)
+        return self._matrix_plan().dense(effective_max_bytes(max_bytes))
+
+    def coo(self, *, max_bytes: Optional[int] = DEFAULT_MAX_BYTES) -> Any:
+        """Deterministic, duplicate-aggregated COO arrays (rows ascending, columns
+        ascending inside a row, exact zeros skipped)."""
+        from ._native_mvp import COOMatrix
+
+        validate_max_bytes(max_bytes)
+        indptr, cols, vals = self._matrix_plan().sparse("coo", effective_max_bytes(max_bytes))
+        dim = 1 << self.nqubits
+        rows = np.repeat(np.arange(dim, dtype=np.uint64), np.diff(indptr.astype(np.int64)))
+        return COOMatrix(rows, cols, vals, (dim, dim))
+
+    def csr(self, *, max_bytes: Optional[int] = DEFAULT_MAX_BYTES) -> Any:
+        """Deterministic CSR arrays from the canonical COO stream."""
+        from ._native_mvp import CSRMatrix
+
+        validate_max_bytes(max_bytes)
+        indptr, cols, vals = self._matrix_plan().sparse("csr", effective_max_bytes(max_bytes))
+        dim = 1 << self.nqubits
+        return CSRMatrix(indptr, cols, vals, (dim, dim))
 
     def backend_mvp_plan(self, *, max_bytes: Optional[int] = DEFAULT_MAX_BYTES) -> Any:
         """Versioned pure-array plan (``pauli.py:953-983`` of the reference)

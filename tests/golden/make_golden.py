@@ -34,6 +34,11 @@ def _codes_from_string(word: str) -> tuple:
     return tuple("IXYZ".index(ch) for ch in word)
 
 
+def _dense_field(n: int, dense: np.ndarray) -> dict:
+    """The reference's dense matrix itself, kept for n <= 6 (pins dense/COO/CSR)."""
+    return {"dense": np.asarray(dense, dtype=np.complex128)} if n <= 6 else {}
+
+
 def main(reference_root: str) -> None:
     sys.path.insert(0, os.path.join(reference_root, "tests"))
     from reference import dense_operator  # the reference's independent oracle
@@ -55,6 +60,7 @@ def main(reference_root: str) -> None:
             coefficients=np.asarray(coefficients, dtype=np.complex128),
             state=state,
             expected=dense @ state,
+            **_dense_field(n, dense),
         )
 
     # random complex differential (test_hamiltonian.py:126-147), same RNG stream
@@ -74,6 +80,7 @@ def main(reference_root: str) -> None:
             coefficients=np.asarray(coefficients, dtype=np.complex128),
             state=state,
             expected=dense @ state,
+            **_dense_field(n, dense),
         )
 
     # qubit ordering (test_hamiltonian.py:71-77): one term on qubit 0 or qubit 2
@@ -87,6 +94,7 @@ def main(reference_root: str) -> None:
                 coefficients=np.asarray([1.0], dtype=np.complex128),
                 state=state,
                 expected=dense @ state,
+                **_dense_field(3, dense),
             )
 
     # ABI fixed vector (test_native_abi.py:84-120): H = 2Z + I on one qubit
@@ -117,6 +125,7 @@ def main(reference_root: str) -> None:
             coefficients=np.asarray(coefficients, dtype=np.complex128),
             state=state,
             expected=dense @ state,
+            **_dense_field(n, dense),
         )
 
     for name, fields in out.items():

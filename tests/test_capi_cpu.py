@@ -34,6 +34,10 @@ def test_library_loads_and_exports_every_declared_symbol() -> None:
     assert set(solver) == set(_native.SOLVER_SYMBOLS)
     for name in solver:
         assert hasattr(lib, name), name
+    matrix = _declared_functions("tcp_matrix.h")
+    assert set(matrix) == set(_native.MATRIX_SYMBOLS)
+    for name in matrix:
+        assert hasattr(lib, name), name
     probe = _declared_functions("tcp_probe.h")
     assert set(probe) == set(_native.PROBE_SYMBOLS)
     for name in probe:
