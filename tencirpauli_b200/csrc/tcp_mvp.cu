@@ -139,7 +139,7 @@ __device__ __forceinline__ void issue_step(const uint4 info, uint64_t tile, cons
 template <int LOGE, typename R>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tiled(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
-            int *__restrict__ err) {
+            int *__restrict__ err, uint64_t tile0) {
     using C = typename Cx<R>::T;
     static_assert(LOGE == 3, "the group dispatch below covers 8 rows per thread");
     constexpr int E = 1 << LOGE;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __shared__ __align__(8) uint64_t bars[2];
 
     const uint32_t tid = threadIdx.x;
-    const uint64_t tile = blockIdx.x;
+    const uint64_t tile = tile0 + blockIdx.x;
     const uint32_t nsteps = s.nsteps;
     const unsigned char *blocks = step_blocks<R>(s);
 
@@ -314,6 +314,7 @@ using tcp::overlaps;
 namespace {
 
 int g_num_sms = 0;
+constexpr uint64_t kHostChunks = 8;  // output-tile chunks of a large host apply
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -383,8 +384,21 @@ template <int LOGE, typename R> int set_smem_attr() {
 }
 
 // Launch one right-hand side.
+// Number of output tiles of the tiled kernel (0 when the plan uses the row
+// kernel for these buffers).
 template <typename R>
-int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t stream) {
+uint64_t tiled_tiles(const tcp_mvp_plan *p, const void *x) {
+    constexpr int LOGE = sizeof(R) == 8 ? kLogRowsC128 : kLogRowsC64;
+    const uint32_t S = kLogThreads + LOGE;
+    const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
+    return (p->nqubits >= S && p->sched.host.tile_bits == S && aligned) ? (p->dim >> S) : 0;
+}
+
+// Apply on `stream`; the tiled kernel writes output tiles [tile0, tile0 +
+// ntiles) (ntiles = 0: all of them).
+template <typename R>
+int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t stream, uint64_t tile0 = 0,
+               uint64_t ntiles = 0) {
     using C = typename Cx<R>::T;
     constexpr bool is64 = sizeof(R) == 8;
     constexpr int LOGE = is64 ? kLogRowsC128 : kLogRowsC64;
@@ -403,10 +417,10 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
                 attr_done[p->device] = true;
             }
         }
-        const uint64_t tiles = p->dim >> S;
+        const uint64_t tiles = ntiles ? ntiles : (p->dim >> S) - tile0;
         const size_t smem = tiled_smem_bytes<LOGE, R>();
         k_tiled<LOGE, R><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
-            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err);
+            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0);
     } else {
         const int threads = 256;
         uint64_t blocks = (p->dim + threads - 1) / threads;
@@ -470,11 +484,55 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         e = cudaMemcpyAsync(ws.x, state, bytes, cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
     }
-    if (!status) status = launch_one<R>(plan, ws.x, ws.y, stream);
-    if (!status) {
-        e = cudaMemcpyAsync(result, ws.y, bytes, cudaMemcpyDeviceToHost, stream);
-        if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+    // Large tiled applies run in kHostChunks launches over consecutive output
+    // tiles; a second stream copies each finished chunk of y to the host while
+    // the next chunk computes, so only the last chunk's copy is exposed.  All
+    // launches and copies are queued before the host waits on any of them.
+    const uint64_t tiles = tiled_tiles<R>(plan, ws.x);
+    const uint64_t chunks = tiles >= kHostChunks * 1024 ? kHostChunks : 1;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t done[kHostChunks] = {};
+    if (!status && chunks > 1) {
+        e = cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking);
+        for (uint64_t c = 0; c < chunks && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&done[c], cudaEventDisableTiming);
+        if (e != cudaSuccess) status = cuda_fail(e, "creating the copy stream");
     }
+    if (!status && chunks > 1) {
+        const uint64_t per = tiles / chunks;
+        for (uint64_t c = 0; c < chunks && !status; ++c) {
+            const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
+            status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
+            if (!status) {
+                e = cudaEventRecord(done[c], stream);
+                if (e != cudaSuccess) status = cuda_fail(e, "chunk event");
+            }
+        }
+        const size_t row_bytes = 2 * sizeof(R);
+        const uint64_t rows_per_tile = plan->dim / tiles;
+        for (uint64_t c = 0; c < chunks && !status; ++c) {
+            const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
+            const size_t off = t0 * rows_per_tile * row_bytes, len = nt * rows_per_tile * row_bytes;
+            e = cudaStreamWaitEvent(copy_stream, done[c], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(reinterpret_cast<unsigned char *>(result) + off,
+                                    static_cast<const unsigned char *>(ws.y) + off, len, cudaMemcpyDeviceToHost,
+                                    copy_stream);
+            if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+        }
+    } else if (!status) {
+        status = launch_one<R>(plan, ws.x, ws.y, stream);
+        if (!status) {
+            e = cudaMemcpyAsync(result, ws.y, bytes, cudaMemcpyDeviceToHost, stream);
+            if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+        }
+    }
+    if (copy_stream) {
+        e = cudaStreamSynchronize(copy_stream);
+        if (!status && e != cudaSuccess) status = cuda_fail(e, "copy stream synchronize");
+        cudaStreamDestroy(copy_stream);
+    }
+    for (auto &ev : done)
+        if (ev) cudaEventDestroy(ev);
     if (stream) {
         e = cudaStreamSynchronize(stream);
         if (!status && e != cudaSuccess) status = cuda_fail(e, "stream synchronize");
@@ -777,7 +835,7 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     if (plan->nqubits >= S && ds.host.tile_bits == S) {
         const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();
         k_tiled<kLogRowsC128, double><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(ds.dev, dx, dy,
-                                                                                                  d_status);
+                                                                                                  d_status, 0);
     } else {
         const int threads = 256;
         const uint64_t blocks = (plan->dim + threads - 1) / threads;

@@ -211,3 +211,25 @@ def test_wrong_device_or_bad_tensor_rejected() -> None:
     with pytest.raises(TypeError):
         plan.apply_device(x, torch.zeros(4, dtype=torch.complex64, device="cuda"))
     assert isinstance(NativeDeviceError("x", 33), RuntimeError)
+
+
+def test_host_apply_of_a_large_state_streams_output_chunks_and_matches_device_path() -> None:
+    """n = 25: the host entry point launches the tiled kernel in chunks of
+    output tiles and copies each chunk back while the next one computes; the
+    result is the same kernel's output, bit for bit."""
+    op = PauliOperator.from_code_arrays(*workloads.random_k_local(n=25, words=64, seed=21))
+    plan = op.native_mvp_plan()
+    x = workloads.random_state_device(25, seed=4)
+    y = torch.empty_like(x)
+    plan.apply_device(x, y)
+    torch.cuda.synchronize()
+    host_x = x.cpu().numpy()
+    out = np.full(1 << 25, np.nan, dtype=np.complex128)
+    plan.apply_into(host_x, out)
+    np.testing.assert_array_equal(out, y.cpu().numpy())
+    pinned_x = torch.from_numpy(host_x).pin_memory()
+    pinned_y = torch.empty_like(pinned_x).pin_memory()
+    plan._native_plan.apply_into(pinned_x.numpy(), pinned_y.numpy(), 2**63 - 1)
+    np.testing.assert_array_equal(pinned_y.numpy(), out)
+    del x, y
+    torch.cuda.empty_cache()
