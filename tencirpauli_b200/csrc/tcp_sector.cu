@@ -401,7 +401,8 @@ __device__ __forceinline__ void cmac(R &ar, R &ai, R &cr, R &ci, R vr, R vi, con
 template <typename R, typename ST, typename IT, int RK, bool SM, bool DIAG>
 __global__ void __launch_bounds__(kU1Threads) k_u1_apply(U1Dev p, U1Apply a, size_t tab_bytes,
                                                          const typename Cplx<R>::T *__restrict__ x,
-                                                         typename Cplx<R>::T *__restrict__ y) {
+                                                         typename Cplx<R>::T *__restrict__ y, uint64_t row0,
+                                                         uint64_t row1) {
     using C = typename Cplx<R>::T;
     using G = GRec<ST>;
     constexpr int U = kU1Unroll;
@@ -443,7 +444,7 @@ __global__ void __launch_bounds__(kU1Threads) k_u1_apply(U1Dev p, U1Apply a, siz
     }
     const ST *basis = static_cast<const ST *>(p.basis);
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < p.dim; i += stride) {
+    for (uint64_t i = row0 + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < row1; i += stride) {
         const ST b = basis[i];
         R ar = 0, ai = 0, cr = 0, ci = 0;
         if (DIAG) {
@@ -725,10 +726,10 @@ std::string bytes_str(unsigned __int128 v) {
 }
 
 template <typename R, typename ST, typename IT, int RK, bool SM, bool DIAG>
-int launch_apply_v(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
+int launch_apply_v(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s, uint64_t row0, uint64_t row1) {
     using C = typename Cplx<R>::T;
     auto kern = k_u1_apply<R, ST, IT, RK, SM, DIAG>;
-    int grid = grid_for(p->dim);
+    int grid = grid_for(row1 - row0);
     size_t smem = 0;
     const size_t tab_bytes = RK ? p->app.ftab_bytes : p->tab_bytes;
     if (SM) {
@@ -741,31 +742,34 @@ int launch_apply_v(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s)
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         grid = std::min<int>(grid, std::max(per_sm, 1) * std::max(g_sms, 1));
     }
-    kern<<<grid, kU1Threads, smem, s>>>(p->dev, p->app, tab_bytes, static_cast<const C *>(x), static_cast<C *>(y));
+    kern<<<grid, kU1Threads, smem, s>>>(p->dev, p->app, tab_bytes, static_cast<const C *>(x), static_cast<C *>(y), row0,
+                                        row1);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "sector MVP kernel launch");
 }
 
 template <typename R, typename ST, typename IT, int RK>
-int launch_apply_t(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
+int launch_apply_t(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s, uint64_t r0, uint64_t r1) {
     const bool diag = p->app.diag != nullptr;
     if (p->smem) {
-        return diag ? launch_apply_v<R, ST, IT, RK, true, true>(p, x, y, s)
-                    : launch_apply_v<R, ST, IT, RK, true, false>(p, x, y, s);
+        return diag ? launch_apply_v<R, ST, IT, RK, true, true>(p, x, y, s, r0, r1)
+                    : launch_apply_v<R, ST, IT, RK, true, false>(p, x, y, s, r0, r1);
     }
-    return diag ? launch_apply_v<R, ST, IT, RK, false, true>(p, x, y, s)
-                : launch_apply_v<R, ST, IT, RK, false, false>(p, x, y, s);
+    return diag ? launch_apply_v<R, ST, IT, RK, false, true>(p, x, y, s, r0, r1)
+                : launch_apply_v<R, ST, IT, RK, false, false>(p, x, y, s, r0, r1);
 }
 
+// Apply on `s` to output rows [row0, row1) (row1 = 0: all rows).
 template <typename R>
-int launch_apply(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s) {
+int launch_apply(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s, uint64_t row0 = 0, uint64_t row1 = 0) {
     if (p->dim == 0) return TCP_OK;
+    if (row1 == 0) row1 = p->dim;
     if (p->basis32) {
-        return p->app.rk == 2 ? launch_apply_t<R, uint32_t, uint32_t, 2>(p, x, y, s)
-                              : launch_apply_t<R, uint32_t, uint32_t, 3>(p, x, y, s);
+        return p->app.rk == 2 ? launch_apply_t<R, uint32_t, uint32_t, 2>(p, x, y, s, row0, row1)
+                              : launch_apply_t<R, uint32_t, uint32_t, 3>(p, x, y, s, row0, row1);
     }
-    if (p->index32) return launch_apply_t<R, uint64_t, uint32_t, 0>(p, x, y, s);
-    return launch_apply_t<R, uint64_t, uint64_t, 0>(p, x, y, s);
+    if (p->index32) return launch_apply_t<R, uint64_t, uint32_t, 0>(p, x, y, s, row0, row1);
+    return launch_apply_t<R, uint64_t, uint64_t, 0>(p, x, y, s, row0, row1);
 }
 
 int count_transitions(const tcp_u1_plan *p, uint64_t *row_counts, uint64_t &total, cudaStream_t s) {
@@ -1139,11 +1143,50 @@ int apply_host(const tcp_u1_plan *plan, const R *state, uint64_t state_len, R *r
         e = cudaMemcpyAsync(dx, state, bytes, cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
     }
-    if (!status) status = launch_apply<R>(plan, dx, dy, stream);
-    if (!status && bytes) {
-        e = cudaMemcpyAsync(result, dy, bytes, cudaMemcpyDeviceToHost, stream);
-        if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+    // Large applies run in kSectorChunks row ranges; a second stream copies
+    // each finished range of y to the host while the next one computes.  All
+    // launches and copies are queued before the host waits on any of them.
+    constexpr uint64_t kSectorChunks = 8;
+    const uint64_t chunks = plan->dim >= (1ull << 22) ? kSectorChunks : 1;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t done[kSectorChunks] = {};
+    if (!status && chunks > 1) {
+        e = cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking);
+        for (uint64_t c = 0; c < chunks && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&done[c], cudaEventDisableTiming);
+        if (e != cudaSuccess) status = cuda_fail(e, "creating the copy stream");
+        const uint64_t per = plan->dim / chunks;
+        for (uint64_t c = 0; c < chunks && !status; ++c) {
+            const uint64_t r0 = c * per, r1 = (c + 1 == chunks) ? plan->dim : r0 + per;
+            status = launch_apply<R>(plan, dx, dy, stream, r0, r1);
+            if (!status) {
+                e = cudaEventRecord(done[c], stream);
+                if (e != cudaSuccess) status = cuda_fail(e, "chunk event");
+            }
+        }
+        for (uint64_t c = 0; c < chunks && !status; ++c) {
+            const uint64_t r0 = c * per, r1 = (c + 1 == chunks) ? plan->dim : r0 + per;
+            const size_t off = r0 * 2 * sizeof(R), len = (r1 - r0) * 2 * sizeof(R);
+            e = cudaStreamWaitEvent(copy_stream, done[c], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(reinterpret_cast<unsigned char *>(result) + off,
+                                    static_cast<const unsigned char *>(dy) + off, len, cudaMemcpyDeviceToHost,
+                                    copy_stream);
+            if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+        }
+    } else if (!status) {
+        status = launch_apply<R>(plan, dx, dy, stream);
+        if (!status && bytes) {
+            e = cudaMemcpyAsync(result, dy, bytes, cudaMemcpyDeviceToHost, stream);
+            if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+        }
     }
+    if (copy_stream) {
+        e = cudaStreamSynchronize(copy_stream);
+        if (!status && e != cudaSuccess) status = cuda_fail(e, "copy stream synchronize");
+        cudaStreamDestroy(copy_stream);
+    }
+    for (auto &ev : done)
+        if (ev) cudaEventDestroy(ev);
     if (stream) {
         e = cudaStreamSynchronize(stream);
         if (!status && e != cudaSuccess) status = cuda_fail(e, "stream synchronize");

@@ -331,3 +331,23 @@ def test_davidson_in_the_half_filling_sector_matches_dense() -> None:
     res = davidson(plan, nev=4, tol=1e-8, seed=2)
     assert res.converged
     np.testing.assert_allclose(res.eigenvalues, ref, atol=1e-9)
+
+
+def test_large_sector_host_apply_streams_output_chunks_and_matches_device_path() -> None:
+    """D = C(26, 13) = 10,400,600: the host entry point runs the sector kernel
+    over row ranges and copies each finished range back while the next one
+    computes; the result equals the device path bit for bit."""
+    op = PauliOperator.from_code_arrays(*workloads.heisenberg_chain(26))
+    plan = op.restrict_charge(U1Sector(26, 13)).mvp_plan()
+    x = workloads.random_state_device(26, seed=8, length=plan.dimension)
+    y = torch.empty_like(x)
+    plan.apply_device(x, y)
+    torch.cuda.synchronize()
+    out = np.full(plan.dimension, np.nan, dtype=np.complex128)
+    plan.apply_into(x.cpu().numpy(), out)
+    np.testing.assert_array_equal(out, y.cpu().numpy())
+    rows = np.sort(np.random.default_rng(2).choice(plan.dimension, size=512, replace=False)).astype(np.uint64)
+    ref = oracle.u1_apply_rows(26, 13, op.x_words, op.z_words, op.coefficients, x.cpu().numpy(), rows)
+    _close(out[rows.astype(np.int64)], ref)
+    del x, y
+    torch.cuda.empty_cache()
