@@ -261,7 +261,7 @@ def run_batched(args: argparse.Namespace) -> None:
     from tencirpauli_b200.batch import BatchedMVP
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    members = workloads.batched_heisenberg_set(args.batch_count, seed=args.seed)
+    members = workloads.batched_heisenberg_set(args.batch_count, seed=args.seed, nmax=args.batch_nmax)
     ops = [PauliOperator.from_code_arrays(c, w) for _, c, w in members]
     plans = [op.native_mvp_plan() for op in ops]
     nrhs = args.batch_rhs
@@ -585,6 +585,7 @@ def main() -> None:
     parser.add_argument("--batch-count", type=int, default=64)
     parser.add_argument("--lattice", default="4x7", help="sector workload: periodic J1-J2 lattice LXxLY")
     parser.add_argument("--batch-rhs", type=int, default=8)
+    parser.add_argument("--batch-nmax", type=int, default=26, help="batched workload: largest member size")
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=10)
     parser.add_argument("--warmup", type=int, default=3)
