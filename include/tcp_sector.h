@@ -14,8 +14,9 @@
  *   v_m(s) = sum_{terms t of m} c_t i^{#Y_t} (-1)^{popcount(z_t & s)},
  *
  * the destination-major form of `aggregate_source` (sector.rs:1051-1127).
- * The device plan covers n <= 64 (one packed word).  Status codes are those
- * of tcp_mvp.h, plus the two PauliError variants of this path.
+ * The device plan covers n <= 256 (states of up to four 64-bit words); the
+ * host rank, unrank and basis entries take any n.  Status codes are those of
+ * tcp_mvp.h, plus the two PauliError variants of this path.
  */
 #ifndef TCP_SECTOR_H
 #define TCP_SECTOR_H

@@ -147,71 +147,76 @@ struct U1Terms {
     int32_t gzero = -1;         // index of the x == 0 group
 };
 
-// compile_terms (sector.rs:926-1021) for n <= 64: groups by x mask in first
-// appearance order, terms in canonical order within a group, weighted
-// coefficient c * i^{#Y} with the textbook complex product (:1034-1049).
+// compile_terms (sector.rs:926-1021): groups by x mask in first appearance
+// order, terms in canonical order within a group, weighted coefficient
+// c * i^{#Y} with the textbook complex product (:1034-1049).  Masks are kept
+// in integer bit space (qubit q is bit n-1-q) as W 64-bit words, least
+// significant word first (W = 1 for n <= 64).
 int compile_u1(uint32_t n, uint64_t count, uint32_t wc, const uint64_t *xw, const uint64_t *zw, const double *coef,
-               U1Terms &out) {
+               uint32_t W, U1Terms &out) {
     uint32_t expected = word_count_of(n);
     if (wc != expected) {
         return fail(TCP_ERR_INVALID_WORD_LENGTH,
                     "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc));
     }
-    if (n > 64) {
-        return fail(TCP_ERR_OVERFLOW, "integer overflow while representing a sector state: the device sector plan "
-                                      "supports at most 64 qubits");
-    }
-    const uint64_t tail = (n % 64) ? ((1ull << (n % 64)) - 1) : ~0ull;
-    std::unordered_map<uint64_t, uint32_t> lookup;
+    std::map<std::vector<uint64_t>, uint32_t> lookup;
     std::vector<uint32_t> group_of(count);
-    std::vector<uint64_t> xm(count), zm(count);
+    std::vector<uint64_t> xm(count * W), zm(count * W);
     std::vector<double> w(2 * count);
     std::vector<uint32_t> counts;
+    std::vector<uint64_t> key(W);
     for (uint64_t t = 0; t < count; ++t) {
         double re = coef[2 * t], im = coef[2 * t + 1];
         if (!std::isfinite(re) || !std::isfinite(im)) {
             return fail(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite");
         }
-        uint64_t xq = n ? (xw[t * wc] & tail) : 0, zq = n ? (zw[t * wc] & tail) : 0;
-        uint64_t x = 0, z = 0;
+        uint32_t ny = 0;
         for (uint32_t q = 0; q < n; ++q) {
-            if ((xq >> q) & 1) x |= 1ull << (n - 1 - q);
-            if ((zq >> q) & 1) z |= 1ull << (n - 1 - q);
+            const bool x = (xw[t * wc + q / 64] >> (q % 64)) & 1, z = (zw[t * wc + q / 64] >> (q % 64)) & 1;
+            const uint32_t e = n - 1 - q;
+            if (x) xm[t * W + e / 64] |= 1ull << (e % 64);
+            if (z) zm[t * W + e / 64] |= 1ull << (e % 64);
+            ny += x && z;
         }
-        const uint32_t ny = static_cast<uint32_t>(__builtin_popcountll(xq & zq)) % 4;
+        ny %= 4;
         double pr = ny == 0 ? 1.0 : (ny == 2 ? -1.0 : 0.0);
         double pi = ny == 1 ? 1.0 : (ny == 3 ? -1.0 : 0.0);
         w[2 * t] = re * pr - im * pi;
         w[2 * t + 1] = re * pi + im * pr;
-        xm[t] = x;
-        zm[t] = z;
-        auto it = lookup.find(x);
+        key.assign(xm.begin() + t * W, xm.begin() + (t + 1) * W);
+        auto it = lookup.find(key);
         uint32_t g;
         if (it == lookup.end()) {
-            g = static_cast<uint32_t>(out.gx.size());
-            lookup.emplace(x, g);
-            out.gx.push_back(x);
+            g = static_cast<uint32_t>(counts.size());
+            lookup.emplace(key, g);
+            bool zero = true;
+            for (uint64_t v : key) {
+                out.gx.push_back(v);
+                out.x_support += __builtin_popcountll(v);
+                zero = zero && v == 0;
+            }
             counts.push_back(0);
-            if (x == 0) out.gzero = static_cast<int32_t>(g);
-            out.x_support += __builtin_popcountll(x);
+            if (zero) out.gzero = static_cast<int32_t>(g);
         } else {
             g = it->second;
         }
         group_of[t] = g;
         ++counts[g];
     }
-    const size_t G = out.gx.size();
+    const size_t G = counts.size();
     out.gt.assign(G + 1, 0);
     for (size_t g = 0; g < G; ++g) out.gt[g + 1] = out.gt[g] + counts[g];
     std::vector<uint32_t> next(out.gt.begin(), out.gt.end() - 1);
-    out.tz.assign(count, 0);
+    out.tz.assign(count * W, 0);
     out.tw.assign(2 * count, 0.0);
     for (uint64_t t = 0; t < count; ++t) {
         uint32_t slot = next[group_of[t]]++;
-        out.tz[slot] = zm[t];
+        for (uint32_t i = 0; i < W; ++i) {
+            out.tz[slot * W + i] = zm[t * W + i];
+            out.z_support += __builtin_popcountll(zm[t * W + i]);
+        }
         out.tw[2 * slot] = w[2 * t];
         out.tw[2 * slot + 1] = w[2 * t + 1];
-        out.z_support += __builtin_popcountll(zm[t]);
     }
     return TCP_OK;
 }
@@ -256,6 +261,24 @@ struct U1Dev {
 // top part and a smaller middle part, L ranks the low bits among words of
 // their own weight.
 constexpr int kU1Unroll = 4;
+
+// Wide plans (64 < n <= 256): states are W 64-bit words in integer bit
+// space, least significant word first; ranks use the 8-bit-chunk tables
+// (read from global memory) and the basis is unranked index by index.  Wide
+// sectors fit in memory only for small k or n - k, so these kernels keep the
+// plain group loop.
+struct U1WDev {
+    const uint64_t *basis;   // [dim * W]
+    const uint64_t *gx;      // [G * W]
+    const uint32_t *gt;      // [G + 1]
+    const uint64_t *tz;      // [T * W]
+    const double2 *tw;       // [T]
+    const float2 *twf;       // [T]
+    const uint64_t *choose;  // [256 * 257] C(e, j), saturated
+    const void *tab;         // IT[nchunk * (kp + 1) * 256]
+    uint64_t dim, tail;      // tail: valid bits of the top word
+    uint32_t n, k, kp, comp, nchunk, ngroups, nterms, pad;
+};
 
 template <typename ST> struct GRec;
 template <> struct GRec<uint32_t> {
@@ -645,6 +668,212 @@ __global__ void k_u1_diag(U1Dev p, int32_t gzero, double2 *out) {
     }
 }
 
+template <int W> struct WState {
+    uint64_t w[W];
+};
+
+template <int W> __device__ __forceinline__ WState<W> wload(const uint64_t *p, uint64_t i) {
+    WState<W> s;
+#pragma unroll
+    for (int q = 0; q < W; ++q) s.w[q] = p[i * W + q];
+    return s;
+}
+template <int W> __device__ __forceinline__ WState<W> wxor(const WState<W> &a, const uint64_t *m) {
+    WState<W> s;
+#pragma unroll
+    for (int q = 0; q < W; ++q) s.w[q] = a.w[q] ^ m[q];
+    return s;
+}
+template <int W> __device__ __forceinline__ uint32_t wpopc(const WState<W> &a) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) c += static_cast<uint32_t>(__popcll(a.w[q]));
+    return c;
+}
+template <int W> __device__ __forceinline__ uint32_t wparity_and(const WState<W> &a, const uint64_t *m) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) c += static_cast<uint32_t>(__popcll(a.w[q] & m[q]));
+    return c & 1u;
+}
+template <int W> __device__ __forceinline__ bool wequal(const WState<W> &a, const WState<W> &b) {
+    bool e = true;
+#pragma unroll
+    for (int q = 0; q < W; ++q) e = e && a.w[q] == b.w[q];
+    return e;
+}
+
+template <int W, typename IT>
+__device__ uint64_t wrank(const WState<W> &s, const U1WDev &d) {
+    const IT *tab = static_cast<const IT *>(d.tab);
+    WState<W> a = s;
+    if (d.comp) {
+#pragma unroll
+        for (int q = 0; q < W; ++q) a.w[q] = ~s.w[q];
+        const uint32_t top = (d.n - 1) / 64;
+        for (int q = 0; q < W; ++q) {
+            if (q > static_cast<int>(top)) a.w[q] = 0;
+        }
+        a.w[top] &= d.tail;
+    }
+    uint64_t r = 0;
+    uint32_t ones = 0;
+    const uint32_t row = d.kp + 1;
+    for (int c = static_cast<int>(d.nchunk) - 1; c >= 0; --c) {
+        const uint32_t v = static_cast<uint32_t>(a.w[c / 8] >> (8 * (c % 8))) & 255u;
+        r += static_cast<uint64_t>(tab[(static_cast<size_t>(c) * row + ones) * 256u + v]);
+        ones += __popc(v);
+    }
+    return d.comp ? d.dim - 1 - r : r;
+}
+
+__device__ __forceinline__ double2 wgroup_value(const U1WDev &d, uint32_t g, const uint64_t *s, int W) {
+    double re = 0, im = 0;
+    for (uint32_t t = d.gt[g]; t < d.gt[g + 1]; ++t) {
+        uint32_t par = 0;
+        for (int q = 0; q < W; ++q) par += static_cast<uint32_t>(__popcll(d.tz[static_cast<size_t>(t) * W + q] & s[q]));
+        const double2 w = d.tw[t];
+        if (par & 1u) {
+            re -= w.x;
+            im -= w.y;
+        } else {
+            re += w.x;
+            im += w.y;
+        }
+    }
+    return make_double2(re, im);
+}
+
+// Basis: one thread per index, unranked from the top integer bit down.
+template <int W>
+__global__ void k_u1w_basis(U1WDev d, uint64_t *__restrict__ out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= d.dim) return;
+    uint64_t r = i, v[W] = {};
+    uint32_t left = d.k;
+    for (int e = static_cast<int>(d.n) - 1; e >= 0 && left; --e) {
+        const uint64_t zero_count = d.choose[static_cast<uint32_t>(e) * 257u + left];  // C(e, left)
+        if (r >= zero_count) {
+            r -= zero_count;
+            v[e / 64] |= 1ull << (e % 64);
+            --left;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < W; ++q) out[i * W + q] = v[q];
+}
+
+template <typename R, int W, typename IT>
+__global__ void k_u1w_apply(U1WDev d, const typename Cplx<R>::T *__restrict__ x, typename Cplx<R>::T *__restrict__ y,
+                            uint64_t row0, uint64_t row1) {
+    using C = typename Cplx<R>::T;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = row0 + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < row1; i += stride) {
+        const WState<W> b = wload<W>(d.basis, i);
+        R ar = 0, ai = 0, cr = 0, ci = 0;
+        for (uint32_t g = 0; g < d.ngroups; ++g) {
+            const WState<W> s = wxor<W>(b, d.gx + static_cast<size_t>(g) * W);
+            if (wpopc<W>(s) != d.k) continue;
+            R vr = 0, vi = 0;
+            for (uint32_t t = d.gt[g]; t < d.gt[g + 1]; ++t) {
+                const C w = sizeof(R) == 8 ? reinterpret_cast<const C *>(d.tw)[t] : reinterpret_cast<const C *>(d.twf)[t];
+                if (wparity_and<W>(s, d.tz + static_cast<size_t>(t) * W)) {
+                    vr -= w.x;
+                    vi -= w.y;
+                } else {
+                    vr += w.x;
+                    vi += w.y;
+                }
+            }
+            if (vr == R(0) && vi == R(0)) continue;
+            const uint64_t j = wequal<W>(s, b) ? i : wrank<W, IT>(s, d);
+            const C xv = x[j];
+            const R pr = vr * xv.x - vi * xv.y, pi = vr * xv.y + vi * xv.x;
+            if (sizeof(R) == 8) {
+                ar += pr;
+                ai += pi;
+            } else {
+                const R yr = pr - cr, yi = pi - ci;
+                const R tr = ar + yr, ti = ai + yi;
+                cr = (tr - ar) - yr;
+                ci = (ti - ai) - yi;
+                ar = tr;
+                ai = ti;
+            }
+        }
+        C out;
+        out.x = ar;
+        out.y = ai;
+        y[i] = out;
+    }
+}
+
+template <int W>
+__global__ void k_u1w_leak(U1WDev d, unsigned long long *first) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < d.dim; i += stride) {
+        const WState<W> b = wload<W>(d.basis, i);
+        for (uint32_t g = 0; g < d.ngroups; ++g) {
+            const WState<W> s = wxor<W>(b, d.gx + static_cast<size_t>(g) * W);
+            if (wpopc<W>(s) == d.k) continue;
+            const double2 v = wgroup_value(d, g, b.w, W);
+            if (v.x != 0.0 || v.y != 0.0) {
+                atomicMin(first, static_cast<unsigned long long>(i * d.ngroups + g));
+                break;
+            }
+        }
+    }
+}
+
+template <int W>
+__global__ void k_u1w_count(U1WDev d, uint64_t *row_counts, unsigned long long *total) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    unsigned long long mine = 0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < d.dim; i += stride) {
+        const WState<W> b = wload<W>(d.basis, i);
+        uint64_t c = 0;
+        for (uint32_t g = 0; g < d.ngroups; ++g) {
+            const WState<W> s = wxor<W>(b, d.gx + static_cast<size_t>(g) * W);
+            if (wpopc<W>(s) != d.k) continue;
+            const double2 v = wgroup_value(d, g, s.w, W);
+            c += (v.x != 0.0 || v.y != 0.0);
+        }
+        if (row_counts) row_counts[i] = c;
+        mine += c;
+    }
+    typedef cub::BlockReduce<unsigned long long, kU1Threads> Reduce;
+    __shared__ typename Reduce::TempStorage tmp;
+    const unsigned long long sum = Reduce(tmp).Sum(mine);
+    if (threadIdx.x == 0 && sum) atomicAdd(total, sum);
+}
+
+template <int W, typename IT>
+__global__ void k_u1w_fill(U1WDev d, const uint64_t *indptr, uint64_t *cols, double2 *vals) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < d.dim; i += stride) {
+        const WState<W> b = wload<W>(d.basis, i);
+        uint64_t pos = indptr[i];
+        for (uint32_t g = 0; g < d.ngroups; ++g) {
+            const WState<W> s = wxor<W>(b, d.gx + static_cast<size_t>(g) * W);
+            if (wpopc<W>(s) != d.k) continue;
+            const double2 v = wgroup_value(d, g, s.w, W);
+            if (v.x == 0.0 && v.y == 0.0) continue;
+            cols[pos] = wequal<W>(s, b) ? i : wrank<W, IT>(s, d);
+            vals[pos] = v;
+            ++pos;
+        }
+    }
+}
+
+template <int W>
+__global__ void k_u1w_diag(U1WDev d, int32_t gzero, double2 *out) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < d.dim; i += stride) {
+        const WState<W> b = wload<W>(d.basis, i);
+        out[i] = gzero < 0 ? make_double2(0.0, 0.0) : wgroup_value(d, static_cast<uint32_t>(gzero), b.w, W);
+    }
+}
+
 int g_sms = 0;
 
 }  // namespace
@@ -659,8 +888,10 @@ struct tcp_u1_plan {
     bool basis32 = true, index32 = true, smem = false;
     size_t tab_bytes = 0, smem_c128 = 0, smem_c64 = 0;
     U1Terms terms;
+    uint32_t W = 1;  // 64-bit words per state (2 or 4 for n > 64)
     U1Dev dev{};
     U1Apply app{};
+    U1WDev wdev{};
     void *block = nullptr;
     size_t block_bytes = 0;
     mutable std::mutex ws_mutex;
@@ -693,7 +924,7 @@ int grid_for(uint64_t rows) {
 // lazy plan, with the choose table of (n + 1) * (active + 1) entries.
 uint64_t estimate_compiled(const tcp_u1_plan *p) {
     const U1Terms &t = p->terms;
-    const uint64_t G = t.gx.size(), T = t.tz.size(), wc = word_count_of(p->n);
+    const uint64_t G = t.gx.size() / p->W, T = t.tz.size() / p->W, wc = word_count_of(p->n);
     unsigned __int128 b = 0;
     b += static_cast<unsigned __int128>(G) * wc * 8 + t.x_support * 8 + static_cast<unsigned __int128>(T) * wc * 8;
     b += static_cast<unsigned __int128>(T) * 16 + (T + 1) * 8 + t.z_support * 8 + G * 40;
@@ -704,8 +935,9 @@ uint64_t estimate_compiled(const tcp_u1_plan *p) {
 // transition_upper_bound + estimate_plan_bytes (sector.rs:1176-1241).
 int estimate_eager(const tcp_u1_plan *p, unsigned __int128 &bytes) {
     unsigned __int128 total = 0;
-    for (uint64_t x : p->terms.gx) {
-        const uint32_t w = static_cast<uint32_t>(__builtin_popcountll(x));
+    for (size_t g = 0; g < p->terms.gx.size() / p->W; ++g) {
+        uint32_t w = 0;
+        for (uint32_t i = 0; i < p->W; ++i) w += static_cast<uint32_t>(__builtin_popcountll(p->terms.gx[g * p->W + i]));
         if (w % 2) continue;
         const uint32_t half = w / 2;
         if (half > p->k || half > p->n - p->k) continue;
@@ -760,10 +992,23 @@ int launch_apply_t(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s,
 }
 
 // Apply on `s` to output rows [row0, row1) (row1 = 0: all rows).
+template <typename R, int W, typename IT>
+int launch_apply_w(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s, uint64_t row0, uint64_t row1) {
+    using C = typename Cplx<R>::T;
+    k_u1w_apply<R, W, IT><<<grid_for(row1 - row0), kU1Threads, 0, s>>>(p->wdev, static_cast<const C *>(x),
+                                                                          static_cast<C *>(y), row0, row1);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "wide sector MVP kernel launch");
+}
+
 template <typename R>
 int launch_apply(const tcp_u1_plan *p, const void *x, void *y, cudaStream_t s, uint64_t row0 = 0, uint64_t row1 = 0) {
     if (p->dim == 0) return TCP_OK;
     if (row1 == 0) row1 = p->dim;
+    if (p->W == 2) return p->index32 ? launch_apply_w<R, 2, uint32_t>(p, x, y, s, row0, row1)
+                                     : launch_apply_w<R, 2, uint64_t>(p, x, y, s, row0, row1);
+    if (p->W == 4) return p->index32 ? launch_apply_w<R, 4, uint32_t>(p, x, y, s, row0, row1)
+                                     : launch_apply_w<R, 4, uint64_t>(p, x, y, s, row0, row1);
     if (p->basis32) {
         return p->app.rk == 2 ? launch_apply_t<R, uint32_t, uint32_t, 2>(p, x, y, s, row0, row1)
                               : launch_apply_t<R, uint32_t, uint32_t, 3>(p, x, y, s, row0, row1);
@@ -778,7 +1023,9 @@ int count_transitions(const tcp_u1_plan *p, uint64_t *row_counts, uint64_t &tota
     if (e != cudaSuccess) return cuda_fail(e, "allocating the transition counter");
     cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s);
     const int grid = grid_for(p->dim);
-    if (p->basis32) k_u1_count<uint32_t><<<grid, kU1Threads, 0, s>>>(p->dev, row_counts, d_total);
+    if (p->W == 2) k_u1w_count<2><<<grid, kU1Threads, 0, s>>>(p->wdev, row_counts, d_total);
+    else if (p->W == 4) k_u1w_count<4><<<grid, kU1Threads, 0, s>>>(p->wdev, row_counts, d_total);
+    else if (p->basis32) k_u1_count<uint32_t><<<grid, kU1Threads, 0, s>>>(p->dev, row_counts, d_total);
     else k_u1_count<uint64_t><<<grid, kU1Threads, 0, s>>>(p->dev, row_counts, d_total);
     unsigned long long h = 0;
     e = cudaGetLastError();
@@ -797,7 +1044,9 @@ int scan_leakage(const tcp_u1_plan *p) {
     if (e != cudaSuccess) return cuda_fail(e, "allocating the leakage flag");
     cudaMemset(d_first, 0xff, sizeof(unsigned long long));
     const int grid = grid_for(p->dim);
-    if (p->basis32) k_u1_leak<uint32_t><<<grid, kU1Threads>>>(p->dev, d_first);
+    if (p->W == 2) k_u1w_leak<2><<<grid, kU1Threads>>>(p->wdev, d_first);
+    else if (p->W == 4) k_u1w_leak<4><<<grid, kU1Threads>>>(p->wdev, d_first);
+    else if (p->basis32) k_u1_leak<uint32_t><<<grid, kU1Threads>>>(p->dev, d_first);
     else k_u1_leak<uint64_t><<<grid, kU1Threads>>>(p->dev, d_first);
     unsigned long long first = 0;
     e = cudaGetLastError();
@@ -805,14 +1054,14 @@ int scan_leakage(const tcp_u1_plan *p) {
     cudaFree(d_first);
     if (e != cudaSuccess) return cuda_fail(e, "scanning for sector leakage");
     if (first == ~0ull) return TCP_OK;
-    const uint64_t G = p->terms.gx.size();
+    const uint64_t G = p->terms.gx.size() / p->W;
     const uint64_t source = first / G, g = first % G;
-    uint64_t word = 0;
-    unrank_packed(p->n, p->k, p->dim, source, &word, word_count_of(p->n));
-    uint64_t b = 0;  // packed qubit word -> integer bits
-    for (uint32_t q = 0; q < p->n; ++q)
-        if ((word >> q) & 1) b |= 1ull << (p->n - 1 - q);
-    const uint32_t actual = static_cast<uint32_t>(__builtin_popcountll(b ^ p->terms.gx[g]));
+    std::vector<uint64_t> words(std::max<uint32_t>(word_count_of(p->n), 1), 0), b(p->W, 0);
+    unrank_packed(p->n, p->k, p->dim, source, words.data(), word_count_of(p->n));
+    for (uint32_t q = 0; q < p->n; ++q)  // packed qubit words -> integer bits
+        if ((words[q / 64] >> (q % 64)) & 1) b[(p->n - 1 - q) / 64] |= 1ull << ((p->n - 1 - q) % 64);
+    uint32_t actual = 0;
+    for (uint32_t i = 0; i < p->W; ++i) actual += static_cast<uint32_t>(__builtin_popcountll(b[i] ^ p->terms.gx[g * p->W + i]));
     return fail(TCP_ERR_SECTOR_LEAKAGE, leak_message(source, p->k, actual));
 }
 
@@ -1105,6 +1354,112 @@ int upload(tcp_u1_plan *p) {
     return TCP_OK;
 }
 
+// Wide plans: one allocation with the saturated C(e, j) table, the 8-bit
+// chunk rank tables, groups, terms and the basis (unranked on the device).
+int upload_wide(tcp_u1_plan *p) {
+    const U1Terms &t = p->terms;
+    const uint32_t W = p->W;
+    const uint32_t G = static_cast<uint32_t>(t.gx.size() / W), T = static_cast<uint32_t>(t.tz.size() / W);
+    std::vector<uint64_t> choose(256 * 257, 0);
+    for (uint32_t a = 0; a < 256; ++a)
+        for (uint32_t b = 0; b <= 256; ++b) {
+            uint64_t c = 0;
+            choose[a * 257 + b] = choose_u64(a, b, c) ? c : ~0ull;
+        }
+    const uint32_t row = p->kp + 1;
+    const size_t entries = static_cast<size_t>(p->nchunk) * row * 256;
+    std::vector<uint64_t> tab(entries, 0);
+    for (uint32_t c = 0; c < p->nchunk; ++c) {
+        const uint32_t below = 8 * c;
+        for (uint32_t a = 0; a < row; ++a) {
+            uint64_t acc = 0;
+            for (uint32_t v = 0; v < 256; ++v) {
+                tab[(static_cast<size_t>(c) * row + a) * 256 + v] = acc;
+                const int need = static_cast<int>(p->kp) - static_cast<int>(a) - __builtin_popcount(v);
+                if (need >= 0 && static_cast<uint32_t>(need) <= below) {
+                    uint64_t cnt = 0;
+                    if (!choose_u64(below, static_cast<uint64_t>(need), cnt) || acc + cnt < acc) acc = ~0ull;
+                    else acc += cnt;
+                }
+            }
+        }
+    }
+    std::vector<uint32_t> tab32;
+    if (p->index32) tab32.assign(tab.begin(), tab.end());
+    std::vector<float> twf(2 * static_cast<size_t>(T));
+    for (size_t i = 0; i < twf.size(); ++i) twf[i] = static_cast<float>(t.tw[i]);
+    struct Piece {
+        const void *src;
+        size_t bytes;
+        size_t off;
+    };
+    Piece pieces[] = {
+        {choose.data(), choose.size() * 8, 0},
+        {p->index32 ? static_cast<const void *>(tab32.data()) : tab.data(), entries * (p->index32 ? 4 : 8), 0},
+        {t.gx.data(), 8ull * t.gx.size(), 0},
+        {t.gt.data(), 4ull * (G + 1), 0},
+        {t.tz.data(), 8ull * t.tz.size(), 0},
+        {t.tw.data(), 16ull * T, 0},
+        {twf.data(), 8ull * T, 0},
+        {nullptr, 8ull * W * p->dim, 0},  // basis, generated on the device
+    };
+    size_t off = 0;
+    for (auto &pc : pieces) {
+        pc.off = off;
+        off += (pc.bytes + 255) / 256 * 256;
+    }
+    void *block = nullptr;
+    cudaError_t e = tcp::injected_alloc_failure() ? cudaErrorMemoryAllocation : cudaMalloc(&block, std::max<size_t>(off, 256));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TCP_ERR_ALLOCATION, "device allocation of the sector plan (" + std::to_string(off) + " bytes) failed");
+    }
+    unsigned char *base = static_cast<unsigned char *>(block);
+    for (auto &pc : pieces) {
+        if (pc.src && pc.bytes) {
+            e = cudaMemcpy(base + pc.off, pc.src, pc.bytes, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(block);
+                return cuda_fail(e, "uploading the sector plan");
+            }
+        }
+    }
+    p->block = block;
+    p->block_bytes = off;
+    p->tab_bytes = entries * (p->index32 ? 4 : 8);
+    U1WDev &d = p->wdev;
+    d.choose = reinterpret_cast<const uint64_t *>(base + pieces[0].off);
+    d.tab = base + pieces[1].off;
+    d.gx = reinterpret_cast<const uint64_t *>(base + pieces[2].off);
+    d.gt = reinterpret_cast<const uint32_t *>(base + pieces[3].off);
+    d.tz = reinterpret_cast<const uint64_t *>(base + pieces[4].off);
+    d.tw = reinterpret_cast<const double2 *>(base + pieces[5].off);
+    d.twf = reinterpret_cast<const float2 *>(base + pieces[6].off);
+    d.basis = reinterpret_cast<const uint64_t *>(base + pieces[7].off);
+    d.dim = p->dim;
+    d.tail = (p->n % 64) ? ((1ull << (p->n % 64)) - 1) : ~0ull;
+    d.n = p->n;
+    d.k = p->k;
+    d.kp = p->kp;
+    d.comp = p->comp;
+    d.nchunk = p->nchunk;
+    d.ngroups = G;
+    d.nterms = T;
+    const unsigned blocks = static_cast<unsigned>((p->dim + kU1Threads - 1) / kU1Threads);
+    uint64_t *basis = reinterpret_cast<uint64_t *>(base + pieces[7].off);
+    if (W == 2) k_u1w_basis<2><<<blocks, kU1Threads>>>(d, basis);
+    else k_u1w_basis<4><<<blocks, kU1Threads>>>(d, basis);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(block);
+        p->block = nullptr;
+        return cuda_fail(e, "generating the wide sector basis");
+    }
+    p->smem = false;
+    return TCP_OK;
+}
+
 template <typename R>
 int apply_host(const tcp_u1_plan *plan, const R *state, uint64_t state_len, R *result, uint64_t result_len) {
     int st = check_u1(plan);
@@ -1331,14 +1686,19 @@ extern "C" int tcp_u1_plan_create(uint32_t nqubits, uint32_t particle_number, ui
     std::unique_ptr<tcp_u1_plan> p(new tcp_u1_plan());
     int st = sector_dimension(nqubits, particle_number, p->dim);
     if (st) return st;
-    st = compile_u1(nqubits, term_count, word_count, x_words, z_words, coefficients, p->terms);
+    if (nqubits > 256) {
+        return fail(TCP_ERR_OVERFLOW, "integer overflow while representing a sector state: the device sector plan "
+                                      "supports at most 256 qubits");
+    }
+    p->W = nqubits <= 64 ? 1 : (nqubits <= 128 ? 2 : 4);
+    st = compile_u1(nqubits, term_count, word_count, x_words, z_words, coefficients, p->W, p->terms);
     if (st) return st;
     p->n = nqubits;
     p->k = particle_number;
     p->kp = std::min(particle_number, nqubits - particle_number);
     p->comp = particle_number > nqubits - particle_number ? 1 : 0;
     p->nchunk = (nqubits + 7) / 8;
-    p->mask = nqubits == 64 ? ~0ull : ((1ull << nqubits) - 1);
+    p->mask = nqubits >= 64 ? ~0ull : ((1ull << nqubits) - 1);
     p->storage = storage;
     p->term_count = term_count;
     p->basis32 = nqubits <= 32;
@@ -1360,7 +1720,7 @@ extern "C" int tcp_u1_plan_create(uint32_t nqubits, uint32_t particle_number, ui
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (g_sms == 0) cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, p->device);
-    st = upload(p.get());
+    st = p->W > 1 ? upload_wide(p.get()) : upload(p.get());
     if (st) return st;
     // Both storages scan every source for leakage once.  The reference's lazy
     // plan finds a leaking group while it applies (aggregate_source); the
@@ -1400,7 +1760,7 @@ extern "C" int tcp_u1_plan_info(const tcp_u1_plan *plan, tcp_u1_plan_info_t *inf
     info->particle_number = plan->k;
     info->dimension = plan->dim;
     info->term_count = plan->term_count;
-    info->group_count = plan->terms.gx.size();
+    info->group_count = plan->terms.gx.size() / plan->W;
     info->storage = plan->storage;
     info->device = plan->device;
     info->transition_count = plan->transitions;
@@ -1446,6 +1806,13 @@ extern "C" int tcp_u1_diagonal_device(const tcp_u1_plan *plan, void *d_diag, uin
     if (len != plan->dim) return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH, "expected structure length " + std::to_string(plan->dim) + ", got " + std::to_string(len));
     if (d_diag == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (plan->W > 1) {
+        double2 *out = static_cast<double2 *>(d_diag);
+        if (plan->W == 2) k_u1w_diag<2><<<grid_for(plan->dim), kU1Threads, 0, s>>>(plan->wdev, plan->terms.gzero, out);
+        else k_u1w_diag<4><<<grid_for(plan->dim), kU1Threads, 0, s>>>(plan->wdev, plan->terms.gzero, out);
+        cudaError_t ew = cudaGetLastError();
+        return ew == cudaSuccess ? TCP_OK : cuda_fail(ew, "wide sector diagonal kernel launch");
+    }
     // the plan holds the diagonal of its x == 0 group (zero when it has none)
     cudaError_t e = plan->app.diag ? cudaMemcpyAsync(d_diag, plan->app.diag, 16 * plan->dim, cudaMemcpyDeviceToDevice, s)
                                    : cudaMemsetAsync(d_diag, 0, 16 * plan->dim, s);
@@ -1514,7 +1881,11 @@ extern "C" int tcp_u1_csr(const tcp_u1_plan *plan, uint64_t *indptr, uint64_t *c
             d_cols2 = d_cols + nnz;
             d_vals2 = d_vals + nnz;
             const int grid = grid_for(D);
-            if (plan->basis32) k_u1_fill<uint32_t, uint32_t><<<grid, kU1Threads>>>(plan->dev, d_indptr, d_cols, d_vals);
+            if (plan->W == 2 && plan->index32) k_u1w_fill<2, uint32_t><<<grid, kU1Threads>>>(plan->wdev, d_indptr, d_cols, d_vals);
+            else if (plan->W == 2) k_u1w_fill<2, uint64_t><<<grid, kU1Threads>>>(plan->wdev, d_indptr, d_cols, d_vals);
+            else if (plan->W == 4 && plan->index32) k_u1w_fill<4, uint32_t><<<grid, kU1Threads>>>(plan->wdev, d_indptr, d_cols, d_vals);
+            else if (plan->W == 4) k_u1w_fill<4, uint64_t><<<grid, kU1Threads>>>(plan->wdev, d_indptr, d_cols, d_vals);
+            else if (plan->basis32) k_u1_fill<uint32_t, uint32_t><<<grid, kU1Threads>>>(plan->dev, d_indptr, d_cols, d_vals);
             else if (plan->index32) k_u1_fill<uint64_t, uint32_t><<<grid, kU1Threads>>>(plan->dev, d_indptr, d_cols, d_vals);
             else k_u1_fill<uint64_t, uint64_t><<<grid, kU1Threads>>>(plan->dev, d_indptr, d_cols, d_vals);
             e = cudaGetLastError();

@@ -277,14 +277,64 @@ def test_many_terms_run_from_global_memory_and_match_oracle() -> None:
     assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= C64_NORM_RTOL
 
 
-def test_single_word_width_boundary_and_wide_sector_error() -> None:
+def test_single_word_width_boundary_and_the_width_limit() -> None:
     # tests/test_symmetry.py:281-286: n = 64, k = 0 (one state)
     op = PauliOperator.from_terms(64, [("I" * 64, 1.0)])
     restricted = op.restrict_charge(U1Sector(64, 0))
     np.testing.assert_allclose(restricted.apply(np.asarray([2.0 + 3.0j])), [2.0 + 3.0j])
-    wide = PauliOperator.from_terms(65, [(_local(65, "X", 63, 64), 0.5), (_local(65, "Y", 63, 64), 0.5)])
-    with pytest.raises(OverflowError, match="at most 64 qubits"):
-        wide.restrict_charge(U1Sector(65, 1))
+    wide = PauliOperator.from_terms(257, [(_local(257, "X", 3, 4), 0.5), (_local(257, "Y", 3, 4), 0.5)])
+    with pytest.raises(OverflowError, match="at most 256 qubits"):
+        wide.restrict_charge(U1Sector(257, 1))
+
+
+def _hopping(n: int, coefficient: complex = 0.5) -> PauliOperator:
+    terms = []
+    for q in range(n - 1):
+        terms += [(_local(n, "X", q, q + 1), coefficient), (_local(n, "Y", q, q + 1), coefficient)]
+    return PauliOperator.from_terms(n, terms)
+
+
+@pytest.mark.parametrize("n,k", [(63, 1), (64, 1), (65, 2), (65, 63), (127, 1), (128, 2), (129, 2), (256, 1)])
+def test_wide_sector_restriction_matches_the_oracle(n: int, k: int) -> None:
+    # the cases of tests/test_u1.py:125-154 of the reference
+    op = _hopping(n)
+    restricted = op.restrict_charge(U1Sector(n, k), storage="eager")
+    indptr, cols, vals = oracle.u1_csr(n, k, op.x_words, op.z_words, op.coefficients)
+    csr = restricted.csr()
+    np.testing.assert_array_equal(csr.indptr, indptr)
+    np.testing.assert_array_equal(csr.indices, cols)
+    assert csr.data.tobytes() == vals.tobytes()
+    rng = np.random.default_rng(n + k)
+    state = rng.normal(size=restricted.dimension) + 1j * rng.normal(size=restricted.dimension)
+    ref = _oracle_apply(op, k, state)
+    _close(restricted.apply(state), ref)
+    _close(op.restrict_charge(U1Sector(n, k)).mvp_plan().apply(state), ref)
+
+
+def test_wide_sector_complex_hopping_across_a_word_boundary_and_leakage() -> None:
+    # tests/test_u1.py:157-199 of the reference: qubits 63 and 64 straddle two words
+    n = 65
+    coefficient = 0.7 + 0.2j
+    op = PauliOperator.from_terms(n, [(_local(n, "X", 63, 64), coefficient), (_local(n, "Y", 63, 64), coefficient),
+                                      (_local(n, "Z", 64), 0.3)])
+    restricted = op.restrict_charge(U1Sector(n, 1), storage="eager")
+    indptr, cols, vals = oracle.u1_csr(n, 1, op.x_words, op.z_words, op.coefficients)
+    csr = restricted.csr()
+    np.testing.assert_array_equal(csr.indices, cols)
+    assert csr.data.tobytes() == vals.tobytes()
+    plan = restricted.mvp_plan(storage="eager")
+    diag = torch.empty(plan.dimension, dtype=torch.complex128, device="cuda")
+    plan.diagonal_device(diag)
+    torch.cuda.synchronize()
+    dense = restricted.dense()
+    np.testing.assert_array_equal(diag.cpu().numpy(), np.diag(dense))
+    leaking = PauliOperator.from_terms(129, [(_local(129, "X", 64), 1.0)])
+    with pytest.raises(ValueError, match=r"U\(1\) sector leakage"):
+        leaking.restrict_charge(U1Sector(129, 1))
+    with pytest.raises(ValueError, match="source index 0: expected particle number 1, got destination weight 2"):
+        leaking.restrict_charge(U1Sector(129, 1), storage="eager")
+    ok = PauliOperator.from_terms(129, [(_local(129, "X", 63, 64), 0.5), (_local(129, "Y", 63, 64), 0.5)])
+    assert ok.restrict_charge(U1Sector(129, 1)).dimension == 129
 
 
 def test_j1j2_4x6_half_filling_equals_the_full_space_plan() -> None:
