@@ -384,6 +384,22 @@ def run_davidson(args: argparse.Namespace) -> None:
             "residuals": [float(v) for v in res.residuals],
             "fallbacks": res.fallbacks,
         }
+    # the same solve inside the half-filling U(1) sector (the ground state and
+    # the low singlets of the even lattice live there): 6x fewer amplitudes
+    from tencirpauli_b200 import U1Sector
+
+    sector_plan = op.restrict_charge(U1Sector(op.nqubits, op.nqubits // 2)).mvp_plan()
+    torch.cuda.synchronize()
+    sres = davidson(sector_plan, nev=4, tol=1e-8, seed=args.seed % 1000, max_iter=args.davidson_max_iter)
+    runs["jacobi_half_filling_sector"] = {
+        "seconds": sres.seconds,
+        "iterations": sres.iterations,
+        "mvps": sres.mvps,
+        "converged": sres.converged,
+        "dimension": sector_plan.dimension,
+        "eigenvalues": [float(v) for v in sres.eigenvalues],
+        "max_abs_diff_vs_full_space": float(max(abs(a - b) for a, b in zip(sres.eigenvalues, runs["jacobi"]["eigenvalues"]))),
+    }
     line = {
         "metric": "Davidson wall time to residual 1e-8 (lowest 4 eigenpairs)",
         "value": runs["learned"]["seconds"],
