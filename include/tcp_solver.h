@@ -36,7 +36,8 @@ int tcp_gram(const void *A, int a_dtype, uint32_t p, const void *B, int b_dtype,
              void *d_G, void *d_work, void *stream);
 
 /* out[:, j] = alpha * sum_i A[:, i] S[i, j] + beta * out[:, j] in FP64
- * arithmetic (S: p x k complex128 column-major on the device, k <= 16). */
+ * arithmetic (S: p x k complex128 column-major on the device, k <= 32,
+ * p * k <= 6144 after k is padded to the next of 4, 8, 16, 32). */
 int tcp_block_combine(const void *A, int a_dtype, uint32_t p, const void *d_S, uint32_t k, uint64_t n,
                       double alpha, double beta, void *out, int out_dtype, void *stream);
 

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <numeric>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -23,10 +24,19 @@ using tcp::fail;
 
 namespace {
 
-constexpr int kGramThreads = 256;
-constexpr int kGramRows = 32;          // rows staged per chunk
+constexpr int kGramThreads = 512;      // 16 warps, one CTA per SM
+constexpr int kGramWarps = kGramThreads / 32;
+constexpr int kGramPairs = 16;         // (i, j) pairs of one warp tile
 constexpr int kGramMaxVectors = 96;    // p + q
-constexpr int kGramBlocks = 296;       // 2 per SM
+constexpr int kGramMaxPairs = 512;     // p * q
+constexpr int kGramBlocks = 296;       // partial-sum slots in the work buffer
+constexpr int kGramGrid = 148;         // CTAs launched (<= kGramBlocks)
+constexpr int kGramRedBytes = 96 * 1024;  // shared memory for the row-group sums
+
+constexpr int kCombineThreads = 256;
+constexpr int kCombineTile = 4;        // output vectors per thread
+constexpr int kCombineUnroll = 8;      // complex128 source vectors loaded ahead (16 for complex64)
+constexpr int kCombineMaxK = 32;       // output vectors per launch
 
 __device__ __forceinline__ double2 load_c(const void *base, int c64, uint64_t idx) {
     if (c64) {
@@ -42,47 +52,131 @@ __device__ __forceinline__ void store_c(void *base, int c64, uint64_t idx, doubl
         static_cast<double2 *>(base)[idx] = v;
     }
 }
+template <bool C64> __device__ __forceinline__ double2 load_v(const void *base, uint64_t idx) {
+    if constexpr (C64) {
+        const float2 v = __ldg(static_cast<const float2 *>(base) + idx);
+        return make_double2(v.x, v.y);
+    } else {
+        return __ldg(static_cast<const double2 *>(base) + idx);
+    }
+}
 
-// Per-block partial sums of conj(A_i) . B_j over a grid-strided set of row
-// chunks; partial[block][i + p*j].
-__global__ void __launch_bounds__(kGramThreads)
-    k_gram_partial(const void *__restrict__ A, int a64, uint32_t p, const void *__restrict__ B, int b64, uint32_t q,
-                   uint64_t n, double2 *__restrict__ partial) {
-    __shared__ double2 sa[kGramRows][kGramMaxVectors];
+// t += conj(a) * b in FP64.
+__device__ __forceinline__ void cmac(double2 &t, double2 a, double2 b) {
+    t.x = fma(a.x, b.x, fma(a.y, b.y, t.x));
+    t.y = fma(a.x, b.y, fma(-a.y, b.x, t.y));
+}
+
+// Per-CTA partial sums of G = A^H B.  The p x q pairs are cut into warp
+// tiles of PI x QJ pairs (PI vectors of A, QJ of B: 8 x 1, 8 x 2 or 4 x 4,
+// at most kGramPairs).  The CTA's rows are dealt to `groups` row groups, and
+// its 16 warps take the (tile, row group) slots in turn: with groups chosen so
+// that slots is a multiple of 16, every warp does the same work.  Warps walk
+// the same 32-row chunks, so the B rows one tile reads are shared through L1
+// by the warps of the other tiles and every vector crosses HBM once.  Each
+// lane keeps its pair sums in FP64 registers; the warp reduces them by a
+// fixed butterfly (commutative steps, so every lane holds the same bits), the
+// row groups of a tile are summed in a fixed order from shared memory, and
+// the CTA writes partial[block][i + p*j].  RPL = 2 (both blocks complex64,
+// n even, 16-byte aligned) gives each lane two rows per chunk.
+template <int QJ, bool A64, bool B64, int RPL>
+__global__ void __launch_bounds__(kGramThreads, 1)
+    k_gram_tiles(const void *__restrict__ A, uint32_t p, const void *__restrict__ B, uint32_t q, uint64_t n,
+                 uint32_t groups, double2 *__restrict__ partial) {
+    constexpr int PI = QJ == 4 ? 4 : 8;
+    constexpr int TP = PI * QJ;
+    static_assert(TP <= kGramPairs, "tile shape");
+    extern __shared__ double2 red[];  // [slot][TP] when groups > 1
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t ni = (p + PI - 1) / PI, nj = (q + QJ - 1) / QJ, ntiles = ni * nj;
+    const uint32_t slots = groups * ntiles;
     const uint32_t pairs = p * q;
-    double2 acc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
-    const uint64_t chunks = (n + kGramRows - 1) / kGramRows;
-    for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-        const uint64_t r0 = c * kGramRows;
-        __syncthreads();
-        for (uint32_t e = threadIdx.x; e < kGramRows * (p + q); e += blockDim.x) {
-            const uint32_t v = e / kGramRows, rr = e % kGramRows;
-            const uint64_t row = r0 + rr;
-            double2 val = make_double2(0.0, 0.0);
-            if (row < n) val = v < p ? load_c(A, a64, v * n + row) : load_c(B, b64, (v - p) * n + row);
-            sa[rr][v] = val;
-        }
-        __syncthreads();
+    const uint64_t chunks = (n + 32 * RPL - 1) / (32 * RPL);
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * groups;
+    for (uint32_t s = warp; s < slots; s += kGramWarps) {
+        const uint32_t tile = s % ntiles, rg = s / ntiles;
+        const uint32_t i0 = (tile % ni) * PI, j0 = (tile / ni) * QJ;
+        double2 acc[TP];
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            const uint32_t pr = threadIdx.x + s * kGramThreads;
-            if (pr < pairs) {
-                const uint32_t i = pr % p, j = pr / p;
-                double re = acc[s].x, im = acc[s].y;
-#pragma unroll 4
-                for (int rr = 0; rr < kGramRows; ++rr) {
-                    const double2 a = sa[rr][i], b = sa[rr][p + j];
-                    re = fma(a.x, b.x, fma(a.y, b.y, re));
-                    im = fma(a.x, b.y, fma(-a.y, b.x, im));
+        for (int e = 0; e < TP; ++e) acc[e] = make_double2(0.0, 0.0);
+        for (uint64_t c = static_cast<uint64_t>(blockIdx.x) * groups + rg; c < chunks; c += stride) {
+            if constexpr (RPL == 1) {
+                const uint64_t row = c * 32 + lane;
+                if (row < n) {
+                    double2 b[QJ], a[PI];
+#pragma unroll
+                    for (int jj = 0; jj < QJ; ++jj)
+                        b[jj] = j0 + jj < q ? load_v<B64>(B, static_cast<uint64_t>(j0 + jj) * n + row)
+                                            : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int ii = 0; ii < PI; ++ii)
+                        a[ii] = i0 + ii < p ? load_v<A64>(A, static_cast<uint64_t>(i0 + ii) * n + row)
+                                            : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int ii = 0; ii < PI; ++ii) {
+#pragma unroll
+                        for (int jj = 0; jj < QJ; ++jj) cmac(acc[ii * QJ + jj], a[ii], b[jj]);
+                    }
                 }
-                acc[s] = make_double2(re, im);
+            } else {
+                // complex64 storage, n even: a lane loads rows 2 lane and
+                // 2 lane + 1 of every vector as one 16-byte float4
+                const uint64_t row = c * 64 + 2 * lane;
+                if (row < n) {
+                    const float4 *A4 = static_cast<const float4 *>(A), *B4 = static_cast<const float4 *>(B);
+                    float4 b[QJ], a[PI];
+#pragma unroll
+                    for (int jj = 0; jj < QJ; ++jj)
+                        b[jj] = j0 + jj < q ? __ldg(B4 + (static_cast<uint64_t>(j0 + jj) * n + row) / 2)
+                                            : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                    for (int ii = 0; ii < PI; ++ii)
+                        a[ii] = i0 + ii < p ? __ldg(A4 + (static_cast<uint64_t>(i0 + ii) * n + row) / 2)
+                                            : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                    for (int ii = 0; ii < PI; ++ii) {
+#pragma unroll
+                        for (int jj = 0; jj < QJ; ++jj) {
+                            cmac(acc[ii * QJ + jj], make_double2(a[ii].x, a[ii].y), make_double2(b[jj].x, b[jj].y));
+                            cmac(acc[ii * QJ + jj], make_double2(a[ii].z, a[ii].w), make_double2(b[jj].z, b[jj].w));
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < TP; ++e) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                acc[e].x += __shfl_xor_sync(0xffffffffu, acc[e].x, off);
+                acc[e].y += __shfl_xor_sync(0xffffffffu, acc[e].y, off);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < TP; ++e) {
+            if (lane == static_cast<uint32_t>(e)) {
+                if (groups == 1u) {
+                    const uint32_t i = i0 + e / QJ, j = j0 + e % QJ;
+                    if (i < p && j < q) partial[static_cast<size_t>(blockIdx.x) * pairs + i + p * j] = acc[e];
+                } else {
+                    red[s * TP + e] = acc[e];
+                }
             }
         }
     }
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        const uint32_t pr = threadIdx.x + s * kGramThreads;
-        if (pr < pairs) partial[static_cast<size_t>(blockIdx.x) * pairs + pr] = acc[s];
+    if (groups > 1u) {
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < ntiles * TP; t += blockDim.x) {
+            const uint32_t tile = t / TP, e = t % TP;
+            double2 sum = make_double2(0.0, 0.0);
+            for (uint32_t rg = 0; rg < groups; ++rg) {
+                const double2 v = red[(rg * ntiles + tile) * TP + e];
+                sum.x += v.x;
+                sum.y += v.y;
+            }
+            const uint32_t i = (tile % ni) * PI + e / QJ, j = (tile / ni) * QJ + e % QJ;
+            if (i < p && j < q) partial[static_cast<size_t>(blockIdx.x) * pairs + i + p * j] = sum;
+        }
     }
 }
 
@@ -100,39 +194,70 @@ __global__ void k_gram_reduce(const double2 *__restrict__ partial, uint32_t bloc
     out[pr] = make_double2(re, im);
 }
 
-// out[:, j] = alpha * sum_i A[:, i] S[i, j] + beta * out[:, j]  (FP64 arithmetic)
-template <int KMAX>
-__global__ void k_combine(const void *__restrict__ A, int a64, uint32_t p, const double2 *__restrict__ S, uint32_t k,
-                          uint64_t n, double alpha, double beta, void *__restrict__ out, int o64) {
-    extern __shared__ double2 ss[];  // S, p x k column-major
-    for (uint32_t e = threadIdx.x; e < p * k; e += blockDim.x) ss[e] = S[e];
+// out[:, j] = alpha * sum_i A[:, i] S[i, j] + beta * out[:, j]  (FP64 arithmetic).
+// A CTA covers rb = 256 / njp consecutive rows for njp tiles of kCombineTile
+// output vectors (njp: the tile count rounded up to a power of two); the
+// tiles of the same rows sit in one CTA, so each source row is fetched from
+// HBM once and re-read from L1.  Source values are loaded 8 (complex128) or
+// 16 (complex64) ahead of their multiply-adds, and every output sums
+// i = 0..p-1 in order.
+// S is staged column-major as p x (njp * kCombineTile), zero beyond k.
+template <bool A64, bool O64>
+__global__ void __launch_bounds__(kCombineThreads)
+    k_combine_tiles(const void *__restrict__ A, uint32_t p, const double2 *__restrict__ S, uint32_t k, uint32_t njp,
+                    uint64_t n, double alpha, double beta, void *__restrict__ out) {
+    extern __shared__ double2 ss[];
+    const uint32_t kpad = njp * kCombineTile;
+    for (uint32_t e = threadIdx.x; e < p * kpad; e += blockDim.x) {
+        const uint32_t j = e / p;
+        ss[e] = j < k ? S[e] : make_double2(0.0, 0.0);
+    }
     __syncthreads();
-    for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; r < n;
-         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        double2 acc[KMAX];
+    const uint32_t rb = kCombineThreads / njp;
+    const uint32_t jt = threadIdx.x / rb;
+    if (jt * kCombineTile >= k) return;  // padding tile: no further barrier below
+    constexpr int U = A64 ? 2 * kCombineUnroll : kCombineUnroll;
+    const double2 *sj = ss + static_cast<size_t>(p) * jt * kCombineTile;
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * rb + threadIdx.x % rb; r < n;
+         r += static_cast<uint64_t>(gridDim.x) * rb) {
+        double2 acc[kCombineTile];
 #pragma unroll
-        for (int j = 0; j < KMAX; ++j) acc[j] = make_double2(0.0, 0.0);
-        for (uint32_t i = 0; i < p; ++i) {
-            const double2 a = load_c(A, a64, i * n + r);
+        for (int jj = 0; jj < kCombineTile; ++jj) acc[jj] = make_double2(0.0, 0.0);
+        uint32_t i = 0;
+        for (; i + U <= p; i += U) {
+            double2 a[U];
 #pragma unroll
-            for (int j = 0; j < KMAX; ++j) {
-                if (j < static_cast<int>(k)) {
-                    const double2 s = ss[i + p * j];
-                    acc[j].x = fma(a.x, s.x, fma(-a.y, s.y, acc[j].x));
-                    acc[j].y = fma(a.x, s.y, fma(a.y, s.x, acc[j].y));
+            for (int u = 0; u < U; ++u) a[u] = load_v<A64>(A, static_cast<uint64_t>(i + u) * n + r);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+#pragma unroll
+                for (int jj = 0; jj < kCombineTile; ++jj) {
+                    const double2 sv = sj[i + u + p * jj];
+                    acc[jj].x = fma(a[u].x, sv.x, fma(-a[u].y, sv.y, acc[jj].x));
+                    acc[jj].y = fma(a[u].x, sv.y, fma(a[u].y, sv.x, acc[jj].y));
                 }
             }
         }
+        for (; i < p; ++i) {
+            const double2 a = load_v<A64>(A, static_cast<uint64_t>(i) * n + r);
 #pragma unroll
-        for (int j = 0; j < KMAX; ++j) {
-            if (j < static_cast<int>(k)) {
-                double2 v = make_double2(alpha * acc[j].x, alpha * acc[j].y);
+            for (int jj = 0; jj < kCombineTile; ++jj) {
+                const double2 sv = sj[i + p * jj];
+                acc[jj].x = fma(a.x, sv.x, fma(-a.y, sv.y, acc[jj].x));
+                acc[jj].y = fma(a.x, sv.y, fma(a.y, sv.x, acc[jj].y));
+            }
+        }
+#pragma unroll
+        for (int jj = 0; jj < kCombineTile; ++jj) {
+            const uint32_t j = jt * kCombineTile + jj;
+            if (j < k) {
+                double2 v = make_double2(alpha * acc[jj].x, alpha * acc[jj].y);
                 if (beta != 0.0) {
-                    const double2 o = load_c(out, o64, j * n + r);
+                    const double2 o = load_c(out, O64, static_cast<uint64_t>(j) * n + r);
                     v.x = fma(beta, o.x, v.x);
                     v.y = fma(beta, o.y, v.y);
                 }
-                store_c(out, o64, j * n + r, v);
+                store_c(out, O64, static_cast<uint64_t>(j) * n + r, v);
             }
         }
     }
@@ -452,6 +577,29 @@ int grid_for(uint64_t n, int threads) {
 
 bool valid_dtype(int d) { return d == TCP_DTYPE_C128 || d == TCP_DTYPE_C64; }
 
+template <int QJ>
+void launch_gram_tiles(int grid, size_t smem, cudaStream_t s, const void *A, bool a64, uint32_t p, const void *B,
+                       bool b64, uint32_t q, uint64_t n, uint32_t groups, bool pairs_of_rows, double2 *partial) {
+#define TCP_GRAM_LAUNCH(A64, B64, RPL)                                                                            \
+    do {                                                                                                        \
+        cudaFuncSetAttribute(k_gram_tiles<QJ, A64, B64, RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                             kGramRedBytes);                                                                    \
+        k_gram_tiles<QJ, A64, B64, RPL><<<grid, kGramThreads, smem, s>>>(A, p, B, q, n, groups, partial);       \
+    } while (0)
+    if (a64 && b64 && pairs_of_rows) {
+        TCP_GRAM_LAUNCH(true, true, 2);
+    } else if (a64 && b64) {
+        TCP_GRAM_LAUNCH(true, true, 1);
+    } else if (a64) {
+        TCP_GRAM_LAUNCH(true, false, 1);
+    } else if (b64) {
+        TCP_GRAM_LAUNCH(false, true, 1);
+    } else {
+        TCP_GRAM_LAUNCH(false, false, 1);
+    }
+#undef TCP_GRAM_LAUNCH
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -465,16 +613,39 @@ extern "C" int tcp_gram(const void *A, int a_dtype, uint32_t p, const void *B, i
                         void *d_G, void *d_work, void *stream) {
     if (!valid_dtype(a_dtype) || !valid_dtype(b_dtype)) return fail(TCP_ERR_INVALID_ARGUMENT, "unknown dtype");
     if (p == 0 || q == 0) return TCP_OK;
-    if (p + q > kGramMaxVectors || p * q > 2 * kGramThreads) {
+    if (p + q > kGramMaxVectors || p * q > kGramMaxPairs) {
         return fail(TCP_ERR_INVALID_ARGUMENT, "tcp_gram supports p + q <= 96 and p * q <= 512");
     }
     if (!A || !B || !d_G || !d_work) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     auto *partial = static_cast<double2 *>(d_work);
-    k_gram_partial<<<kGramBlocks, kGramThreads, 0, s>>>(A, a_dtype == TCP_DTYPE_C64, p, B, b_dtype == TCP_DTYPE_C64, q,
-                                                        n, partial);
+    const uint32_t qj = q == 1 ? 1u : (q == 2 ? 2u : 4u);
+    const uint32_t pi = qj == 4 ? 4u : 8u;  // tile shape of k_gram_tiles<qj>
+    const uint32_t ntiles = ((p + pi - 1) / pi) * ((q + qj - 1) / qj);
+    // Row groups per CTA: slots = ntiles * groups = lcm(ntiles, 16) keeps all
+    // 16 warps equally busy; if those partial sums do not fit in shared
+    // memory, fall back to 16 / ntiles groups (or one).
+    const uint32_t tp = pi * qj;
+    uint32_t groups = kGramWarps / std::gcd(ntiles, static_cast<uint32_t>(kGramWarps));
+    if (static_cast<size_t>(groups) * ntiles * tp * sizeof(double2) > static_cast<size_t>(kGramRedBytes))
+        groups = ntiles >= static_cast<uint32_t>(kGramWarps) ? 1u : kGramWarps / ntiles;
+    const size_t smem = groups > 1 ? static_cast<size_t>(groups) * ntiles * tp * sizeof(double2) : 0;
+    const bool a64 = a_dtype == TCP_DTYPE_C64, b64 = b_dtype == TCP_DTYPE_C64;
+    const bool pairs_of_rows = a64 && b64 && n % 2 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0 &&
+                               reinterpret_cast<uintptr_t>(B) % 16 == 0;
+    const uint64_t rows_per_chunk = pairs_of_rows ? 64 : 32;
+    const uint64_t chunks = (n + rows_per_chunk - 1) / rows_per_chunk;
+    const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(kGramGrid, (chunks + groups - 1) / groups)));
+    if (qj == 1) {
+        launch_gram_tiles<1>(grid, smem, s, A, a64, p, B, b64, q, n, groups, pairs_of_rows, partial);
+    } else if (qj == 2) {
+        launch_gram_tiles<2>(grid, smem, s, A, a64, p, B, b64, q, n, groups, pairs_of_rows, partial);
+    } else {
+        launch_gram_tiles<4>(grid, smem, s, A, a64, p, B, b64, q, n, groups, pairs_of_rows, partial);
+    }
     const uint32_t pairs = p * q;
-    k_gram_reduce<<<(pairs + 127) / 128, 128, 0, s>>>(partial, kGramBlocks, pairs, static_cast<double2 *>(d_G));
+    k_gram_reduce<<<(pairs + 127) / 128, 128, 0, s>>>(partial, static_cast<uint32_t>(grid), pairs,
+                                                      static_cast<double2 *>(d_G));
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "gram kernel launch");
 }
@@ -483,27 +654,32 @@ extern "C" int tcp_block_combine(const void *A, int a_dtype, uint32_t p, const v
                                  double alpha, double beta, void *out, int out_dtype, void *stream) {
     if (!valid_dtype(a_dtype) || !valid_dtype(out_dtype)) return fail(TCP_ERR_INVALID_ARGUMENT, "unknown dtype");
     if (k == 0) return TCP_OK;
-    if (k > 16) return fail(TCP_ERR_INVALID_ARGUMENT, "tcp_block_combine supports k <= 16");
-    if (p * k * sizeof(double2) > 96 * 1024) return fail(TCP_ERR_INVALID_ARGUMENT, "coefficient block too large");
+    if (k > static_cast<uint32_t>(kCombineMaxK)) return fail(TCP_ERR_INVALID_ARGUMENT, "tcp_block_combine supports k <= 32");
+    uint32_t njp = 1;
+    while (njp * kCombineTile < k) njp <<= 1;
+    const size_t smem = static_cast<size_t>(p) * njp * kCombineTile * sizeof(double2);
+    if (smem > 96 * 1024) return fail(TCP_ERR_INVALID_ARGUMENT, "coefficient block too large");
     if (!A || !d_S || !out) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    if (n == 0) return TCP_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const size_t smem = p * k * sizeof(double2);
-    const int threads = 256;
-    const int grid = grid_for(n, threads);
-    const int a64 = a_dtype == TCP_DTYPE_C64, o64 = out_dtype == TCP_DTYPE_C64;
+    const uint32_t rb = kCombineThreads / njp;
+    const int grid = static_cast<int>(std::min<uint64_t>((n + rb - 1) / rb, 148ull * 8));
+    const bool a64 = a_dtype == TCP_DTYPE_C64, o64 = out_dtype == TCP_DTYPE_C64;
     const auto *S = static_cast<const double2 *>(d_S);
-    cudaError_t e;
-    if (k <= 4) {
-        cudaFuncSetAttribute(k_combine<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        k_combine<4><<<grid, threads, smem, s>>>(A, a64, p, S, k, n, alpha, beta, out, o64);
-    } else if (k <= 8) {
-        cudaFuncSetAttribute(k_combine<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        k_combine<8><<<grid, threads, smem, s>>>(A, a64, p, S, k, n, alpha, beta, out, o64);
+    if (a64 && o64) {
+        cudaFuncSetAttribute(k_combine_tiles<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_combine_tiles<true, true><<<grid, kCombineThreads, smem, s>>>(A, p, S, k, njp, n, alpha, beta, out);
+    } else if (a64) {
+        cudaFuncSetAttribute(k_combine_tiles<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_combine_tiles<true, false><<<grid, kCombineThreads, smem, s>>>(A, p, S, k, njp, n, alpha, beta, out);
+    } else if (o64) {
+        cudaFuncSetAttribute(k_combine_tiles<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_combine_tiles<false, true><<<grid, kCombineThreads, smem, s>>>(A, p, S, k, njp, n, alpha, beta, out);
     } else {
-        cudaFuncSetAttribute(k_combine<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        k_combine<16><<<grid, threads, smem, s>>>(A, a64, p, S, k, n, alpha, beta, out, o64);
+        cudaFuncSetAttribute(k_combine_tiles<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_combine_tiles<false, false><<<grid, kCombineThreads, smem, s>>>(A, p, S, k, njp, n, alpha, beta, out);
     }
-    e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "combine kernel launch");
 }
 

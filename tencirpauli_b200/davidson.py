@@ -59,13 +59,15 @@ class JacobiPreconditioner:
         return True
 
 
-def _orthonormalize(T: Any, drop: float) -> Any:
+def _orthonormalize(T: Any, drop: float, G: Any = None) -> Any:
     """Orthonormal basis of span(T) (rows are vectors) by an eigen-
-    decomposition of the FP64 Gram matrix; directions with relative weight
-    below `drop` are discarded."""
+    decomposition of the FP64 Gram matrix (`G`, when the caller has it on the
+    host already); directions with relative weight below `drop` are
+    discarded."""
     import torch
 
-    G = solver_ops.gram(T, T).to("cpu")
+    if G is None:
+        G = solver_ops.gram(T, T).to("cpu")
     G = (G + G.conj().T) / 2
     w, Q = torch.linalg.eigh(G)
     keep = w > drop * max(float(w.max()), 1e-300)
@@ -142,13 +144,15 @@ def davidson(
             evals, evecs = torch.linalg.eigh(Th)
             theta = evals[:nev].clone()
             S = evecs[:, :nev]
-            U = torch.empty((nev, n), dtype=dtype, device="cuda")
-            HU = torch.empty_like(U)
-            solver_ops.combine(V[:m], S, U)
-            solver_ops.combine(W[:m], S, HU)
-            R = HU.clone()
-            solver_ops.combine(U, -torch.diag(theta.to(torch.complex128)), R, beta=1.0)
+            # residuals R = W S - V S diag(theta): one pass over V and one over W
+            R = torch.empty((nev, n), dtype=dtype, device="cuda")
+            solver_ops.combine(V[:m], -S * theta.to(torch.complex128), R)
+            solver_ops.combine(W[:m], S, R, beta=1.0)
             norms = torch.sqrt(torch.clamp(torch.diagonal(solver_ops.gram(R, R)).real, min=0.0)).cpu().numpy()
+            U = None
+            if callback is not None:
+                U = torch.empty((nev, n), dtype=dtype, device="cuda")
+                solver_ops.combine(V[:m], S, U)
             iterations += 1
             phase_it += 1
             if record_history:
@@ -163,6 +167,9 @@ def davidson(
             done = bool((norms <= phase_tol).all())
             stalled = dtype == torch.complex64 and stall >= 15
             if done or stalled or iterations >= max_iter:
+                if U is None:
+                    U = torch.empty((nev, n), dtype=dtype, device="cuda")
+                    solver_ops.combine(V[:m], S, U)
                 if dtype == torch.complex64:
                     # hand the lowest `keep` Ritz vectors to the FP64 phase
                     carry = min(keep, m)
@@ -176,7 +183,8 @@ def davidson(
             if not ok or not bool(torch.isfinite(torch.view_as_real(Tc)).all()):
                 fallbacks += 1
                 solver_ops.jacobi(Rsel, diag, theta[idx], Tc)
-            if m + Tc.shape[0] > max_subspace:
+            restarted = m + Tc.shape[0] > max_subspace
+            if restarted:
                 # thick restart on the lowest `keep` Ritz vectors
                 Sk = evecs[:, :keep]
                 Vn = torch.empty((keep, n), dtype=dtype, device="cuda")
@@ -189,10 +197,27 @@ def davidson(
                 m = keep
                 Tm.zero_()
                 Tm[:m, :m] = torch.diag(evals[:keep].to(torch.complex128))
-            for _ in range(2):  # classical Gram-Schmidt, twice
+            # Block classical Gram-Schmidt against V with the DGKS test: with V
+            # orthonormal, |t|^2 = |c|^2 + |t - V c|^2, and a second sweep runs
+            # only when a sweep removed more than half of a column's squared
+            # norm (|t - V c|^2 < |c|^2).
+            for _ in range(2):
                 C = solver_ops.gram(V[:m], Tc)
                 solver_ops.combine(V[:m], C, Tc, alpha=-1.0, beta=1.0)
-            new = _orthonormalize(Tc, drop)
+                G = solver_ops.gram(Tc, Tc).to("cpu")
+                removed = (C.abs() ** 2).sum(dim=0).cpu()
+                if bool((torch.diagonal(G).real >= removed).all()):
+                    break
+            new = _orthonormalize(Tc, drop, G)
+            if new.shape[0] == 0:
+                # no new direction: keep the current Ritz vectors (after a
+                # restart they are the first nev basis vectors)
+                if U is None:
+                    U = V[:nev].clone() if restarted else torch.empty((nev, n), dtype=dtype, device="cuda")
+                    if not restarted:
+                        solver_ops.combine(V[:m], S, U)
+                if dtype == torch.complex64:
+                    X = U
         phase_iterations.append(phase_it)
         if dtype != torch.complex64:
             X = U

@@ -102,15 +102,19 @@ def gram(A: Any, B: Any, stream: Any = None) -> Any:
 
 def combine(A: Any, S: Any, out: Any, alpha: float = 1.0, beta: float = 0.0, stream: Any = None) -> Any:
     """out[j] = alpha * sum_i A[i] S[i, j] + beta * out[j] (FP64 arithmetic);
-    more than 16 output vectors are done 16 at a time."""
+    the outputs go 32 at a time (fewer when p is so large that p x 32
+    coefficients do not fit one launch's shared-memory block)."""
     import torch
 
     p, n = _vectors(A)
     k, n2 = _vectors(out)
     if n != n2 or tuple(S.shape) != (p, k):
         raise ValueError("shape mismatch in combine")
-    for j0 in range(0, k, 16):
-        j1 = min(k, j0 + 16)
+    step = 32
+    while step > 4 and p * step > 6144:
+        step //= 2
+    for j0 in range(0, k, step):
+        j1 = min(k, j0 + step)
         Sc = S[:, j0:j1].to(device=A.device, dtype=torch.complex128).transpose(0, 1).contiguous()  # column-major
         o = out[j0:j1]
         _native.raise_for_status(

@@ -57,6 +57,42 @@ def test_gram_and_combine_match_fp64_numpy(adt) -> None:
     np.testing.assert_allclose(out.cpu().numpy(), expect, rtol=1e-12, atol=1e-10)
 
 
+@pytest.mark.parametrize(
+    "p,q,adt,bdt",
+    [
+        (1, 1, torch.complex128, torch.complex128),  # one 8 x 1 tile, 16 row groups
+        (9, 2, torch.complex64, torch.complex64),  # 8 x 2 tiles, ragged in p
+        (64, 4, torch.complex128, torch.complex64),  # 16 tiles: one per warp
+        (68, 4, torch.complex64, torch.complex128),  # 17 tiles: a second round
+        (32, 16, torch.complex128, torch.complex128),  # 8 x 4 tiles
+        (5, 7, torch.complex64, torch.complex64),  # q padded to 8
+    ],
+)
+def test_gram_tile_shapes_match_fp64_numpy(p, q, adt, bdt) -> None:
+    n = 4099  # not a multiple of the 32-row chunk
+    A = _rand((p, n), adt, 11 + p)
+    B = _rand((q, n), bdt, 13 + q)
+    G = solver_ops.gram(A, B).cpu().numpy()
+    expect = A.cpu().numpy().astype(np.complex128).conj() @ B.cpu().numpy().astype(np.complex128).T
+    np.testing.assert_allclose(G, expect, rtol=1e-12, atol=1e-10)
+    assert np.array_equal(G, solver_ops.gram(A, B).cpu().numpy())  # fixed reduction order
+
+
+@pytest.mark.parametrize("p,k,adt,odt", [(3, 1, torch.complex128, torch.complex64), (13, 9, torch.complex64, torch.complex64),
+                                          (64, 32, torch.complex128, torch.complex128), (40, 20, torch.complex64, torch.complex128),
+                                          (300, 40, torch.complex128, torch.complex128)])
+def test_combine_tile_shapes_match_fp64_numpy(p, k, adt, odt) -> None:
+    n = 1031
+    A = _rand((p, n), adt, 17 + p)
+    S = torch.complex(torch.randn(p, k, dtype=torch.float64), torch.randn(p, k, dtype=torch.float64))
+    out = _rand((k, n), odt, 19 + k)
+    before = out.cpu().numpy().astype(np.complex128)
+    solver_ops.combine(A, S, out, alpha=-1.0, beta=1.0)
+    expect = before - S.numpy().T @ A.cpu().numpy().astype(np.complex128)
+    tol = 1e-12 if odt == torch.complex128 else 2e-6
+    np.testing.assert_allclose(out.cpu().numpy(), expect, rtol=tol, atol=tol * np.abs(expect).max())
+
+
 def test_features_inputs_and_corrections_match_oracle() -> None:
     op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(3, 4, 1.0, 0.4))
     plan = op.native_mvp_plan()
