@@ -591,13 +591,73 @@ def run_sector(args: argparse.Namespace) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_solver(args: argparse.Namespace) -> None:
+    """The two vector kernels of the Davidson solver at its sizes: the FP64
+    Gram C = V^H T and the update T -= V C of block Gram-Schmidt, for a
+    64-vector basis V and a 4-vector block T of length n (2^24 for the 4x6
+    lattice), in complex128 and complex64 storage.  Bandwidth counts the
+    algorithmic bytes of one launch: Gram reads V and T; the update reads V
+    and T and writes T.  V alone (64 vectors) exceeds L2, so no flush is
+    needed between launches."""
+    import torch
+
+    from tencirpauli_b200 import solver_ops
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, p, q = args.solver_n, 64, 4
+    peaks = _measured_peaks()
+    results = {}
+    for name in (["c128", "c64"] if args.solver_dtype == "both" else [args.solver_dtype]):
+        dtype = torch.complex128 if name == "c128" else torch.complex64
+        es = 16 if name == "c128" else 8
+        g = torch.Generator(device="cuda")
+        g.manual_seed(args.seed % 1000)
+        V = torch.randn((p, n), dtype=dtype, device="cuda", generator=g)
+        T = torch.randn((q, n), dtype=dtype, device="cuda", generator=g)
+        C = solver_ops.gram(V, T)
+        for _ in range(args.warmup):
+            solver_ops.gram(V, T)
+            solver_ops.combine(V, C, T, alpha=-1.0, beta=1.0)
+        torch.cuda.synchronize()
+        times = {}
+        for op in ("gram", "combine"):
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(args.steps):
+                if op == "gram":
+                    solver_ops.gram(V, T)
+                else:
+                    solver_ops.combine(V, C, T, alpha=-1.0, beta=1.0)
+            end.record()
+            torch.cuda.synchronize()
+            times[op] = start.elapsed_time(end) / args.steps
+        gram_bytes = (p + q) * n * es
+        comb_bytes = (p + 2 * q) * n * es
+        results[name] = {
+            "gram_ms": times["gram"], "gram_gbs": gram_bytes / times["gram"] / 1e6,
+            "combine_ms": times["combine"], "combine_gbs": comb_bytes / times["combine"] / 1e6,
+            "gram_bytes": gram_bytes, "combine_bytes": comb_bytes,
+        }
+        del V, T
+        torch.cuda.empty_cache()
+    first = next(iter(results.values()))
+    print(json.dumps({
+        "metric": "Davidson Gram / block-combine bandwidth", "value": first["gram_gbs"], "unit": "GB/s",
+        "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+        "config": {"workload": f"basis of {p} vectors x block of {q}, length {n}", "l2": "inputs larger than L2"},
+        "peak_hbm_gbs": peaks["hbm_gbs"], "peak_source": peaks["source"], "results": results,
+    }), flush=True)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--weights", default=None)
     parser.add_argument("--train", action="store_true")
     parser.add_argument("--davidson-max-iter", type=int, default=600)
-    parser.add_argument("--workload", choices=["random28", "batched", "davidson", "chemistry", "sector"],
+    parser.add_argument("--workload", choices=["random28", "batched", "davidson", "chemistry", "sector", "solver"],
                         default="random28")
+    parser.add_argument("--solver-n", type=int, default=1 << 24, help="solver workload: vector length")
+    parser.add_argument("--solver-dtype", choices=["both", "c128", "c64"], default="both")
     parser.add_argument("--batch-count", type=int, default=64)
     parser.add_argument("--lattice", default="4x7", help="sector workload: periodic J1-J2 lattice LXxLY")
     parser.add_argument("--batch-rhs", type=int, default=8)
@@ -631,6 +691,9 @@ def main() -> None:
         return
     if args.workload == "sector":
         run_sector(args)
+        return
+    if args.workload == "solver":
+        run_solver(args)
         return
 
     import torch
