@@ -5,12 +5,15 @@
 //
 // Vectors are stored RHS-major (vector v at offset v * n) as complex64 or
 // complex128; every reduction and combination accumulates in FP64.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
-#include <numeric>
 #include <cstring>
+#include <numeric>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -32,6 +35,8 @@ constexpr int kGramMaxPairs = 512;     // p * q
 constexpr int kGramBlocks = 296;       // partial-sum slots in the work buffer
 constexpr int kGramGrid = 148;         // CTAs launched (<= kGramBlocks)
 constexpr int kGramRedBytes = 96 * 1024;  // shared memory for the row-group sums
+constexpr int kGramStages = 4;            // TMA pipeline depth (chunks)
+constexpr uint32_t kGramStageBytes = 48 * 1024;  // one chunk of every vector
 
 constexpr int kCombineThreads = 256;
 constexpr int kCombineTile = 4;        // output vectors per thread
@@ -60,6 +65,8 @@ template <bool C64> __device__ __forceinline__ double2 load_v(const void *base, 
         return __ldg(static_cast<const double2 *>(base) + idx);
     }
 }
+
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
 // t += conj(a) * b in FP64.
 __device__ __forceinline__ void cmac(double2 &t, double2 a, double2 b) {
@@ -177,6 +184,161 @@ __global__ void __launch_bounds__(kGramThreads, 1)
             const uint32_t i = (tile % ni) * PI + e / QJ, j = (tile / ni) * QJ + e % QJ;
             if (i < p && j < q) partial[static_cast<size_t>(blockIdx.x) * pairs + i + p * j] = sum;
         }
+    }
+}
+
+// 2-D tiled TMA load of one box (x: innermost coordinate in 8-byte units,
+// y: vector index) into shared memory; completes the box bytes on `bar`.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// G = A^H B for two blocks of the same storage type, fed by the TMA engine.
+// The blocks are described by two 2-D tensor maps (vectors x 8-byte units),
+// and a chunk is one box of each: `rows` rows of every vector.  A CTA walks
+// its full chunks (chunk c = blockIdx.x + k * gridDim.x) through a
+// kGramStages-deep ring in shared memory; thread 0 issues the two box loads
+// of a chunk onto the stage's mbarrier kGramStages - 1 chunks ahead of the
+// consumers, so the loads in flight hold no registers.  The last n % rows
+// rows are read straight from global memory by the CTA next in turn.  Warp w
+// takes tile w % ntiles and row group w / ntiles (ntiles * groups <= 16); its
+// lanes keep the tile's pair sums in FP64 registers.  The reduction order is
+// fixed (warp butterfly, row groups, then k_gram_reduce over CTAs).  A box
+// that does not land within the bounded wait poisons this CTA's partial sums
+// with NaN, after a bounded wait for the boxes still in flight, so the caller
+// sees a non-finite Gram matrix.
+template <int QJ, bool C64>
+__global__ void __launch_bounds__(kGramThreads, 1)
+    k_gram_tma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+               const void *__restrict__ A, uint32_t p, const void *__restrict__ B, uint32_t q, uint64_t n,
+               uint32_t rows, uint32_t groups, double2 *__restrict__ partial) {
+    using E = std::conditional_t<C64, float2, double2>;
+    constexpr int PI = QJ == 4 ? 4 : 8;
+    constexpr int TP = PI * QJ;
+    constexpr int UNITS = sizeof(E) / 8;  // 8-byte units per element
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[kGramStages];
+    __shared__ double2 red[kGramWarps][kGramPairs];
+    E *ring = reinterpret_cast<E *>(smem_raw);
+    const uint32_t vecs = p + q;
+    const size_t stage_elems = static_cast<size_t>(vecs) * rows;
+    const uint32_t stage_bytes = static_cast<uint32_t>(stage_elems * sizeof(E));
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t ni = (p + PI - 1) / PI, nj = (q + QJ - 1) / QJ, ntiles = ni * nj;
+    const uint32_t pairs = p * q;
+    const uint64_t chunks = n / rows;  // full chunks only
+    const uint64_t mine = chunks > blockIdx.x ? (chunks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+
+    if (tid == 0) {
+        for (int st = 0; st < kGramStages; ++st) mbar_init(&full[st], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    // chunk k of this CTA -> stage k % kGramStages
+    auto issue = [&](uint64_t k) {
+        const uint64_t r0 = (blockIdx.x + k * gridDim.x) * static_cast<uint64_t>(rows);
+        uint64_t *bar = &full[k % kGramStages];
+        E *dst = ring + (k % kGramStages) * stage_elems;
+        mbar_arrive_expect_tx(bar, stage_bytes);
+        tma_load_2d(dst, &ta, static_cast<int>(r0 * UNITS), 0, bar);
+        tma_load_2d(dst + static_cast<size_t>(p) * rows, &tb, static_cast<int>(r0 * UNITS), 0, bar);
+    };
+    if (tid == 0) {
+        for (uint64_t k = 0; k < mine && k + 1 < static_cast<uint64_t>(kGramStages); ++k) issue(k);
+    }
+
+    const bool active = warp < ntiles * groups;
+    const uint32_t tile = warp % ntiles, rg = warp / ntiles;
+    const uint32_t i0 = (tile % ni) * PI, j0 = (tile / ni) * QJ;
+    double2 acc[TP];
+#pragma unroll
+    for (int e = 0; e < TP; ++e) acc[e] = make_double2(0.0, 0.0);
+    // one row of the tile's vectors, from shared memory or from global memory
+    auto accumulate = [&](const E *sa, const E *sb, size_t stride, uint64_t r) {
+        double2 a[PI], b[QJ];
+#pragma unroll
+        for (int jj = 0; jj < QJ; ++jj) {
+            if (j0 + jj < q) {
+                const E v = sb[(j0 + jj) * stride + r];
+                b[jj] = make_double2(v.x, v.y);
+            } else {
+                b[jj] = make_double2(0.0, 0.0);
+            }
+        }
+#pragma unroll
+        for (int ii = 0; ii < PI; ++ii) {
+            if (i0 + ii < p) {
+                const E v = sa[(i0 + ii) * stride + r];
+                a[ii] = make_double2(v.x, v.y);
+            } else {
+                a[ii] = make_double2(0.0, 0.0);
+            }
+        }
+#pragma unroll
+        for (int ii = 0; ii < PI; ++ii) {
+#pragma unroll
+            for (int jj = 0; jj < QJ; ++jj) cmac(acc[ii * QJ + jj], a[ii], b[jj]);
+        }
+    };
+    for (uint64_t k = 0; k < mine; ++k) {
+        const uint32_t st = static_cast<uint32_t>(k % kGramStages);
+        const bool ok = mbar_wait_bounded(&full[st], static_cast<uint32_t>(k / kGramStages) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                // let the boxes already issued land before the CTA exits
+                const uint64_t issued = umin64(mine, k + kGramStages - 1);
+                for (uint64_t kk = k; kk < issued; ++kk)
+                    mbar_wait_bounded(&full[kk % kGramStages], static_cast<uint32_t>(kk / kGramStages) & 1u,
+                                      kWaitLimitNs / 4);
+            }
+            const double nan = __longlong_as_double(0x7ff8000000000000ll);
+            for (uint32_t pr = tid; pr < pairs; pr += blockDim.x)
+                partial[static_cast<size_t>(blockIdx.x) * pairs + pr] = make_double2(nan, nan);
+            return;
+        }
+        // every thread has finished chunk k - 1, so its stage can be refilled
+        if (tid == 0 && k + kGramStages - 1 < mine) {
+            fence_proxy_async_smem();
+            issue(k + kGramStages - 1);
+        }
+        if (active) {
+            const E *sa = ring + st * stage_elems;
+            for (uint32_t r = rg * 32 + lane; r < rows; r += groups * 32) accumulate(sa, sa + static_cast<size_t>(p) * rows, rows, r);
+        }
+    }
+    const uint64_t tail0 = chunks * rows;
+    if (active && tail0 < n && blockIdx.x == chunks % gridDim.x) {
+        for (uint64_t r = tail0 + rg * 32 + lane; r < n; r += groups * 32)
+            accumulate(static_cast<const E *>(A), static_cast<const E *>(B), n, r);
+    }
+#pragma unroll
+    for (int e = 0; e < TP; ++e) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            acc[e].x += __shfl_xor_sync(0xffffffffu, acc[e].x, off);
+            acc[e].y += __shfl_xor_sync(0xffffffffu, acc[e].y, off);
+        }
+    }
+    if (active) {
+#pragma unroll
+        for (int e = 0; e < TP; ++e)
+            if (lane == static_cast<uint32_t>(e)) red[warp][e] = acc[e];
+    }
+    __syncthreads();
+    for (uint32_t t = tid; t < ntiles * TP; t += blockDim.x) {
+        const uint32_t tl = t / TP, e = t % TP;
+        double2 sum = make_double2(0.0, 0.0);
+        for (uint32_t g = 0; g < groups; ++g) {
+            const double2 v = red[g * ntiles + tl][e];
+            sum.x += v.x;
+            sum.y += v.y;
+        }
+        const uint32_t i = (tl % ni) * PI + e / QJ, j = (tl / ni) * QJ + e % QJ;
+        if (i < p && j < q) partial[static_cast<size_t>(blockIdx.x) * pairs + i + p * j] = sum;
     }
 }
 
@@ -600,6 +762,79 @@ void launch_gram_tiles(int grid, size_t smem, cudaStream_t s, const void *A, boo
 #undef TCP_GRAM_LAUNCH
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult qres;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &qres) != cudaSuccess ||
+            qres != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+        }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }();
+    return fn;
+}
+
+// Tensor map of `vecs` vectors of length n (element size es) seen as a 2-D
+// array of 8-byte units; box = `rows` rows of every vector.
+bool vector_block_map(CUtensorMap *map, const void *base, uint32_t vecs, uint64_t n, size_t es, uint32_t rows) {
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {n * (es / 8), vecs};
+    const cuuint64_t strides[1] = {n * es};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(rows * (es / 8)), vecs};
+    const cuuint32_t elem_strides[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims, strides, box, elem_strides,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA-fed Gram for two complex128 blocks: 16-byte aligned vectors, at
+// most 16 warp tiles, n * 8-byte units below 2^31.  Returns false (nothing
+// launched) when those conditions do not hold.  Complex64 blocks take the
+// register-fed kernel, which measured faster for them (3.1 against 2.6 TB/s
+// at n = 2^24 with 64 + 4 vectors; both are bound by FP64 work, 16 FMAs and
+// 2 conversions per 8-byte value), while complex128 gains 5.2 -> 5.7 TB/s.
+// (The kernel template also reads complex64 blocks with n even.)
+bool launch_gram_tma(const void *A, bool a64, uint32_t p, const void *B, bool b64, uint32_t q, uint64_t n,
+                     uint32_t qj, uint32_t ntiles, cudaStream_t s, double2 *partial, uint32_t *grid_used) {
+    if (a64 || b64 || ntiles > static_cast<uint32_t>(kGramWarps)) return false;
+    const size_t es = a64 ? sizeof(float2) : sizeof(double2);
+    if ((n * es) % 16 != 0 || n * (es / 8) >= (1ull << 31) || reinterpret_cast<uintptr_t>(A) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(B) % 16 != 0)
+        return false;
+    const uint32_t vecs = p + q;
+    // rows per chunk: a multiple of 32, one stage <= kGramStageBytes, a box
+    // edge <= 256 units
+    uint32_t rows = static_cast<uint32_t>(kGramStageBytes / (vecs * es)) / 32u * 32u;
+    rows = std::min<uint32_t>(rows, static_cast<uint32_t>(256 / (es / 8)));
+    if (rows < 32) return false;
+    CUtensorMap ta, tb;
+    if (!vector_block_map(&ta, A, p, n, es, rows) || !vector_block_map(&tb, B, q, n, es, rows)) return false;
+    const uint32_t groups = std::max<uint32_t>(1u, std::min<uint32_t>(kGramWarps / ntiles, rows / 32u));
+    const uint64_t chunks = n / rows;
+    const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(kGramGrid, chunks)));
+    const size_t smem = static_cast<size_t>(kGramStages) * vecs * rows * es;
+#define TCP_GRAM_TMA(QJ, C64)                                                                                   \
+    do {                                                                                                      \
+        cudaFuncSetAttribute(k_gram_tma<QJ, C64>, cudaFuncAttributeMaxDynamicSharedMemorySize,                 \
+                             static_cast<int>(kGramStages * kGramStageBytes));                                \
+        k_gram_tma<QJ, C64><<<grid, kGramThreads, smem, s>>>(ta, tb, A, p, B, q, n, rows, groups, partial);   \
+    } while (0)
+    if (qj == 1) {
+        TCP_GRAM_TMA(1, false);
+    } else if (qj == 2) {
+        TCP_GRAM_TMA(2, false);
+    } else {
+        TCP_GRAM_TMA(4, false);
+    }
+#undef TCP_GRAM_TMA
+    *grid_used = static_cast<uint32_t>(grid);
+    return true;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -622,15 +857,23 @@ extern "C" int tcp_gram(const void *A, int a_dtype, uint32_t p, const void *B, i
     const uint32_t qj = q == 1 ? 1u : (q == 2 ? 2u : 4u);
     const uint32_t pi = qj == 4 ? 4u : 8u;  // tile shape of k_gram_tiles<qj>
     const uint32_t ntiles = ((p + pi - 1) / pi) * ((q + qj - 1) / qj);
-    // Row groups per CTA: slots = ntiles * groups = lcm(ntiles, 16) keeps all
-    // 16 warps equally busy; if those partial sums do not fit in shared
-    // memory, fall back to 16 / ntiles groups (or one).
+    const bool a64 = a_dtype == TCP_DTYPE_C64, b64 = b_dtype == TCP_DTYPE_C64;
+    uint32_t grid_used = 0;
+    if (launch_gram_tma(A, a64, p, B, b64, q, n, qj, ntiles, s, partial, &grid_used)) {
+        const uint32_t pairs = p * q;
+        k_gram_reduce<<<(pairs + 127) / 128, 128, 0, s>>>(partial, grid_used, pairs, static_cast<double2 *>(d_G));
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? TCP_OK : cuda_fail(e, "gram kernel launch");
+    }
+    // Register-fed tiles (mixed storage types, odd complex64 lengths, more
+    // than 16 tiles).  Row groups per CTA: slots = ntiles * groups =
+    // lcm(ntiles, 16) keeps all 16 warps equally busy; if those partial sums
+    // do not fit in shared memory, fall back to 16 / ntiles groups (or one).
     const uint32_t tp = pi * qj;
     uint32_t groups = kGramWarps / std::gcd(ntiles, static_cast<uint32_t>(kGramWarps));
     if (static_cast<size_t>(groups) * ntiles * tp * sizeof(double2) > static_cast<size_t>(kGramRedBytes))
         groups = ntiles >= static_cast<uint32_t>(kGramWarps) ? 1u : kGramWarps / ntiles;
     const size_t smem = groups > 1 ? static_cast<size_t>(groups) * ntiles * tp * sizeof(double2) : 0;
-    const bool a64 = a_dtype == TCP_DTYPE_C64, b64 = b_dtype == TCP_DTYPE_C64;
     const bool pairs_of_rows = a64 && b64 && n % 2 == 0 && reinterpret_cast<uintptr_t>(A) % 16 == 0 &&
                                reinterpret_cast<uintptr_t>(B) % 16 == 0;
     const uint64_t rows_per_chunk = pairs_of_rows ? 64 : 32;

@@ -141,6 +141,9 @@ def davidson(
             execution.apply_device(V[m : m + k], W[m : m + k])
             mvps += k
             G = solver_ops.gram(V[: m + k], W[m : m + k]).to("cpu")  # (m+k) x k
+            if not bool(torch.isfinite(G).all()):
+                # the Gram kernels return NaN when a bounded device wait expires
+                raise RuntimeError("non-finite projected matrix (device wait timed out, or NaN/Inf in H x)")
             Tm[: m + k, m : m + k] = G
             Tm[m : m + k, :m] = G[:m].conj().T
             m += k

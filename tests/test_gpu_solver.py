@@ -58,23 +58,26 @@ def test_gram_and_combine_match_fp64_numpy(adt) -> None:
 
 
 @pytest.mark.parametrize(
-    "p,q,adt,bdt",
+    "p,q,adt,bdt,n",
     [
-        (1, 1, torch.complex128, torch.complex128),  # one 8 x 1 tile, 16 row groups
-        (9, 2, torch.complex64, torch.complex64),  # 8 x 2 tiles, ragged in p
-        (64, 4, torch.complex128, torch.complex64),  # 16 tiles: one per warp
-        (68, 4, torch.complex64, torch.complex128),  # 17 tiles: a second round
-        (32, 16, torch.complex128, torch.complex128),  # 8 x 4 tiles
-        (5, 7, torch.complex64, torch.complex64),  # q padded to 8
+        (1, 1, torch.complex128, torch.complex128, 4099),  # TMA: one 8 x 1 tile, 4 row groups, 3-row tail
+        (9, 2, torch.complex64, torch.complex64, 4099),  # register tiles, odd length
+        (64, 4, torch.complex128, torch.complex64, 4099),  # mixed storage: register tiles, one per warp
+        (68, 4, torch.complex64, torch.complex128, 4099),  # 17 register tiles
+        (32, 16, torch.complex128, torch.complex128, 4099),  # 32 tiles: register tiles, two rounds
+        (5, 7, torch.complex64, torch.complex64, 4100),  # register tiles, q padded to 8
+        (64, 4, torch.complex64, torch.complex64, 150002),  # register tiles, two rows per lane
+        (52, 4, torch.complex128, torch.complex128, 100003),  # TMA: 13 tiles, several chunks per CTA, tail
+        (13, 1, torch.complex128, torch.complex128, 65536),  # TMA: no tail
+        (20, 2, torch.complex64, torch.complex64, 70000),
     ],
 )
-def test_gram_tile_shapes_match_fp64_numpy(p, q, adt, bdt) -> None:
-    n = 4099  # not a multiple of the 32-row chunk
+def test_gram_tile_shapes_match_fp64_numpy(p, q, adt, bdt, n) -> None:
     A = _rand((p, n), adt, 11 + p)
     B = _rand((q, n), bdt, 13 + q)
     G = solver_ops.gram(A, B).cpu().numpy()
     expect = A.cpu().numpy().astype(np.complex128).conj() @ B.cpu().numpy().astype(np.complex128).T
-    np.testing.assert_allclose(G, expect, rtol=1e-12, atol=1e-10)
+    np.testing.assert_allclose(G, expect, rtol=1e-12, atol=1e-10 * np.sqrt(n / 4099))
     assert np.array_equal(G, solver_ops.gram(A, B).cpu().numpy())  # fixed reduction order
 
 
