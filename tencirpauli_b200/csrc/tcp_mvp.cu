@@ -136,10 +136,13 @@ __device__ __forceinline__ void issue_step(const uint4 info, uint64_t tile, cons
 // Tile-staged grouped MVP (see file header).  Grid: one CTA per output tile;
 // thread t owns rows t + j * kThreads of the tile.  Shared memory: two source
 // tiles and two step blocks (double buffering), refilled by the TMA engine.
-template <int LOGE, typename R>
+// PASSES = false runs every step and overwrites y.  PASSES = true runs pass
+// `pass` (0..3): only the steps whose source tiles lie in quarter `pass` of
+// the state (see DevSchedule::pass_begin), adding to y when `accumulate`.
+template <int LOGE, typename R, bool PASSES>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tiled(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
-            int *__restrict__ err, uint64_t tile0) {
+            int *__restrict__ err, uint64_t tile0, uint32_t pass, uint32_t accumulate) {
     using C = typename Cx<R>::T;
     static_assert(LOGE == 3, "the group dispatch below covers 8 rows per thread");
     constexpr int E = 1 << LOGE;
@@ -152,7 +155,17 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const uint32_t tid = threadIdx.x;
     const uint64_t tile = tile0 + blockIdx.x;
-    const uint32_t nsteps = s.nsteps;
+    uint32_t step0 = 0, nsteps = s.nsteps;
+    if constexpr (PASSES) {
+        // constant indices only: a computed index into the parameter struct
+        // would copy it to the stack
+        const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.pass_shift)) & 3u;
+        const uint32_t* pb = s.pass_begin;
+        step0 = v == 0u ? pb[0] : (v == 1u ? pb[1] : (v == 2u ? pb[2] : pb[3]));
+        const uint32_t step1 = v == 0u ? pb[1] : (v == 1u ? pb[2] : (v == 2u ? pb[3] : pb[4]));
+        nsteps = step1 - step0;
+    }
+    const uint4 *steps = s.step_info + step0;
     const unsigned char *blocks = step_blocks<R>(s);
 
     if (tid == 0) {
@@ -161,12 +174,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0 && nsteps > 0) issue_step<C, S>(__ldg(&s.step_info[0]), tile, x, blocks, tiles, blks, &bars[0]);
+    if (tid == 0 && nsteps > 0) issue_step<C, S>(__ldg(&steps[0]), tile, x, blocks, tiles, blks, &bars[0]);
 
     Acc<R> acc[E];
     for (uint32_t st = 0; st < nsteps; ++st) {
         const uint32_t b = st & 1u;
-        const uint4 info = __ldg(&s.step_info[st]);
+        const uint4 info = __ldg(&steps[st]);
         const bool ok = mbar_wait_bounded(&bars[b], (st >> 1) & 1u);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicOr(err, kErrTimeout);
@@ -175,7 +188,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // Every thread has finished step st-1, so the other buffers are free.
         if (tid == 0 && st + 1 < nsteps) {
             fence_proxy_async_smem();
-            issue_step<C, S>(__ldg(&s.step_info[st + 1]), tile, x, blocks, tiles + (b ^ 1u) * TILE,
+            issue_step<C, S>(__ldg(&steps[st + 1]), tile, x, blocks, tiles + (b ^ 1u) * TILE,
                              blks + (b ^ 1u) * tcp::kBlockBytesMax, &bars[b ^ 1u]);
         }
         const C *xs = tiles + b * TILE;
@@ -197,8 +210,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     }
     C *yt = y + (tile << S);
+    if (PASSES && accumulate) {
 #pragma unroll
-    for (int j = 0; j < E; ++j) yt[tid + (j << kLogThreads)] = acc[j].value();
+        for (int j = 0; j < E; ++j) {
+            C &out = yt[tid + (j << kLogThreads)];
+            const C v = acc[j].value();
+            out.x += v.x;
+            out.y += v.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < E; ++j) yt[tid + (j << kLogThreads)] = acc[j].value();
+    }
 }
 
 // One thread per row; gathers straight from global memory.
@@ -318,6 +341,27 @@ constexpr uint64_t kHostChunks = 8;  // output-tile chunks of a large host apply
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Step ranges of the source-chunk passes (see DevSchedule::pass_begin): the
+// top two bits v of each step's outer pattern d, which is non-decreasing in
+// step order because steps are sorted by d.
+void set_passes(DevSchedule &dev, const tcp::Schedule &h, uint32_t nqubits) {
+    const uint32_t nsteps = static_cast<uint32_t>(h.step_info.size() / 4);
+    dev.pass_shift = kNoPasses;
+    for (int v = 0; v < 5; ++v) dev.pass_begin[v] = v == 0 ? 0u : nsteps;
+    if (nqubits < h.tile_bits + 2) return;
+    const uint32_t shift = nqubits - h.tile_bits - 2;
+    uint32_t prev = 0;
+    for (uint32_t st = 0; st < nsteps; ++st) {
+        const uint64_t d = static_cast<uint64_t>(h.step_info[4 * st]) | (static_cast<uint64_t>(h.step_info[4 * st + 1]) << 32);
+        const uint32_t v = static_cast<uint32_t>(d >> shift);
+        if (v > 3 || v < prev) return;  // not a sorted schedule: no passes
+        for (uint32_t w = prev + 1; w <= v; ++w) dev.pass_begin[w] = st;
+        prev = v;
+    }
+    for (uint32_t w = prev + 1; w <= 4; ++w) dev.pass_begin[w] = nsteps;
+    dev.pass_shift = shift;
+}
+
 // Lay both schedules out in one device allocation.
 int upload(tcp_mvp_plan *p) {
     struct Piece {
@@ -340,6 +384,7 @@ int upload(tcp_mvp_plan *p) {
         add(h.t_wf.data(), h.t_wf.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wf));
         ds->dev.nsteps = static_cast<uint32_t>(h.step_info.size() / 4);
         ds->dev.tile_bits = h.tile_bits;
+        set_passes(ds->dev, h, p->nqubits);
         ds->dev.ngroups = static_cast<uint32_t>(h.g_mask.size());
     }
     size_t total = 256;  // error word first
@@ -378,8 +423,11 @@ template <int LOGE, typename R> constexpr size_t tiled_smem_bytes() {
 
 template <int LOGE, typename R> int set_smem_attr() {
     constexpr size_t bytes = tiled_smem_bytes<LOGE, R>();
-    cudaError_t e = cudaFuncSetAttribute(k_tiled<LOGE, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_tiled<LOGE, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(bytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tiled<LOGE, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(bytes));
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "cudaFuncSetAttribute");
 }
 
@@ -398,7 +446,7 @@ uint64_t tiled_tiles(const tcp_mvp_plan *p, const void *x) {
 // ntiles) (ntiles = 0: all of them).
 template <typename R>
 int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t stream, uint64_t tile0 = 0,
-               uint64_t ntiles = 0) {
+               uint64_t ntiles = 0, int pass = -1, bool accumulate = false) {
     using C = typename Cx<R>::T;
     constexpr bool is64 = sizeof(R) == 8;
     constexpr int LOGE = is64 ? kLogRowsC128 : kLogRowsC64;
@@ -419,8 +467,14 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
         }
         const uint64_t tiles = ntiles ? ntiles : (p->dim >> S) - tile0;
         const size_t smem = tiled_smem_bytes<LOGE, R>();
-        k_tiled<LOGE, R><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
-            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0);
+        if (pass >= 0) {
+            k_tiled<LOGE, R, true><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, static_cast<uint32_t>(pass),
+                accumulate ? 1u : 0u);
+        } else {
+            k_tiled<LOGE, R, false><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, 0u);
+        }
     } else {
         const int threads = 256;
         uint64_t blocks = (p->dim + threads - 1) / threads;
@@ -480,28 +534,59 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     int status = TCP_OK;
     if (e != cudaSuccess) status = cuda_fail(e, "cudaStreamCreate");
-    if (!status) {
-        e = cudaMemcpyAsync(ws.x, state, bytes, cudaMemcpyHostToDevice, stream);
-        if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
-    }
-    // Large tiled applies run in kHostChunks launches over consecutive output
-    // tiles; a second stream copies each finished chunk of y to the host while
-    // the next chunk computes, so only the last chunk's copy is exposed.  All
-    // launches and copies are queued before the host waits on any of them.
+    // Large tiled applies overlap both copies with the kernel.
+    //  * Input: the state goes in as four quarters on its own stream.  Pass k
+    //    (k = 0..3) waits for quarter k only and runs the steps whose source
+    //    tiles lie in it (k_tiled's `pass`), adding to y after the first, so
+    //    the copy of quarters 1..3 overlaps passes 0..2.
+    //  * Output: the last pass runs in kHostChunks launches over consecutive
+    //    output tiles; a third stream copies each finished chunk of y to the
+    //    host while the next chunk computes.
+    // All copies and launches are queued before the host waits on any of
+    // them.  Smaller applies copy, launch once and copy back on one stream.
     const uint64_t tiles = tiled_tiles<R>(plan, ws.x);
     const uint64_t chunks = tiles >= kHostChunks * 1024 ? kHostChunks : 1;
-    cudaStream_t copy_stream = nullptr;
+    const bool passes = chunks > 1 && plan->sched.dev.pass_shift != kNoPasses;
+    constexpr int kQuarters = 4;
+    cudaStream_t copy_stream = nullptr, in_stream = nullptr;
     cudaEvent_t done[kHostChunks] = {};
+    cudaEvent_t landed[kQuarters] = {};
     if (!status && chunks > 1) {
         e = cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking);
         for (uint64_t c = 0; c < chunks && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&done[c], cudaEventDisableTiming);
-        if (e != cudaSuccess) status = cuda_fail(e, "creating the copy stream");
+        if (passes && e == cudaSuccess) e = cudaStreamCreateWithFlags(&in_stream, cudaStreamNonBlocking);
+        for (int k = 0; passes && k < kQuarters && e == cudaSuccess; ++k)
+            e = cudaEventCreateWithFlags(&landed[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) status = cuda_fail(e, "creating the copy streams");
+    }
+    if (!status && passes) {
+        const size_t quarter = bytes / kQuarters;
+        for (int k = 0; k < kQuarters && !status; ++k) {
+            e = cudaMemcpyAsync(static_cast<unsigned char *>(ws.x) + k * quarter,
+                                reinterpret_cast<const unsigned char *>(state) + k * quarter, quarter,
+                                cudaMemcpyHostToDevice, in_stream);
+            if (e == cudaSuccess) e = cudaEventRecord(landed[k], in_stream);
+            if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
+        }
+    } else if (!status) {
+        e = cudaMemcpyAsync(ws.x, state, bytes, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
     }
     if (!status && chunks > 1) {
+        for (int k = 0; passes && k < kQuarters - 1 && !status; ++k) {
+            e = cudaStreamWaitEvent(stream, landed[k], 0);
+            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input quarter");
+            if (!status) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
+        }
+        if (!status && passes) {
+            e = cudaStreamWaitEvent(stream, landed[kQuarters - 1], 0);
+            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input quarter");
+        }
         const uint64_t per = tiles / chunks;
         for (uint64_t c = 0; c < chunks && !status; ++c) {
             const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
-            status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
+            status = passes ? launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, kQuarters - 1, true)
+                            : launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
             if (!status) {
                 e = cudaEventRecord(done[c], stream);
                 if (e != cudaSuccess) status = cuda_fail(e, "chunk event");
@@ -526,12 +611,15 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
             if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
         }
     }
-    if (copy_stream) {
-        e = cudaStreamSynchronize(copy_stream);
+    for (cudaStream_t side : {in_stream, copy_stream}) {
+        if (!side) continue;
+        e = cudaStreamSynchronize(side);
         if (!status && e != cudaSuccess) status = cuda_fail(e, "copy stream synchronize");
-        cudaStreamDestroy(copy_stream);
+        cudaStreamDestroy(side);
     }
     for (auto &ev : done)
+        if (ev) cudaEventDestroy(ev);
+    for (auto &ev : landed)
         if (ev) cudaEventDestroy(ev);
     if (stream) {
         e = cudaStreamSynchronize(stream);
@@ -834,8 +922,8 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     const uint32_t S = kTileBitsC128;
     if (plan->nqubits >= S && ds.host.tile_bits == S) {
         const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();
-        k_tiled<kLogRowsC128, double><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(ds.dev, dx, dy,
-                                                                                                  d_status, 0);
+        k_tiled<kLogRowsC128, double, false><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(
+            ds.dev, dx, dy, d_status, 0, 0u, 0u);
     } else {
         const int threads = 256;
         const uint64_t blocks = (plan->dim + threads - 1) / threads;

@@ -214,10 +214,17 @@ def test_wrong_device_or_bad_tensor_rejected() -> None:
 
 
 def test_host_apply_of_a_large_state_streams_output_chunks_and_matches_device_path() -> None:
-    """n = 25: the host entry point launches the tiled kernel in chunks of
-    output tiles and copies each chunk back while the next one computes; the
-    result is the same kernel's output, bit for bit."""
-    op = PauliOperator.from_code_arrays(*workloads.random_k_local(n=25, words=64, seed=21))
+    """n = 25: the host entry point copies the state in quarters and runs one
+    pass of the tiled kernel per quarter (the steps whose source tiles lie in
+    it, adding to y after the first), then splits the last pass into chunks
+    of output tiles whose copies overlap the next chunk.  Only the grouping
+    of the FP64 sums differs from the single-pass device apply; pageable and
+    pinned host buffers give the same bits."""
+    codes, coeffs = workloads.random_k_local(n=25, words=64, seed=21)
+    # X or Y letters on the two top row bits (qubits 0 and 1) put steps into
+    # more than one pass
+    assert np.isin(codes[:, 0], (1, 2)).any() and np.isin(codes[:, 1], (1, 2)).any()
+    op = PauliOperator.from_code_arrays(codes, coeffs)
     plan = op.native_mvp_plan()
     x = workloads.random_state_device(25, seed=4)
     y = torch.empty_like(x)
@@ -226,10 +233,19 @@ def test_host_apply_of_a_large_state_streams_output_chunks_and_matches_device_pa
     host_x = x.cpu().numpy()
     out = np.full(1 << 25, np.nan, dtype=np.complex128)
     plan.apply_into(host_x, out)
-    np.testing.assert_array_equal(out, y.cpu().numpy())
+    dev = y.cpu().numpy()
+    assert np.linalg.norm(out - dev) <= 1e-14 * np.linalg.norm(dev)
+    rows = np.random.default_rng(5).choice(1 << 25, 256, replace=False).astype(np.uint64)
+    xm, zm, wp = oracle.matrix_terms(op.nqubits, op.x_words, op.z_words, op.coefficients)
+    expect = oracle.apply_rows(25, xm, zm, wp, host_x, rows)
+    np.testing.assert_allclose(out[rows.astype(np.int64)], expect, rtol=1e-12, atol=1e-12 * np.abs(expect).max())
     pinned_x = torch.from_numpy(host_x).pin_memory()
     pinned_y = torch.empty_like(pinned_x).pin_memory()
     plan._native_plan.apply_into(pinned_x.numpy(), pinned_y.numpy(), 2**63 - 1)
     np.testing.assert_array_equal(pinned_y.numpy(), out)
+    # complex64 host buffers take the same passes with Kahan-compensated sums
+    out64 = np.empty(1 << 25, dtype=np.complex64)
+    plan._native_plan.apply_c64_into(host_x.astype(np.complex64), out64)
+    assert np.linalg.norm(out64 - dev) <= 2e-6 * np.linalg.norm(dev)
     del x, y
     torch.cuda.empty_cache()
