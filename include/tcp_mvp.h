@@ -135,6 +135,12 @@ int tcp_mvp_plan_info(const tcp_mvp_plan *plan, tcp_mvp_plan_info_t *info);
  * Lengths are in complex elements; a length other than 2^n returns
  * TCP_ERR_INVALID_STRUCTURE_LENGTH ("expected structure length E, got A").
  * max_bytes is accepted and ignored, as in the reference (hamiltonian.rs:223).
+ * States of 2^25 or more amplitudes (8192 output tiles) are copied in
+ * quarters, each followed by the kernel pass that reads it, and copied back
+ * in chunks of output tiles while later chunks compute; page-locked host
+ * buffers let the copies overlap the kernel.  The FP64 sums are then grouped
+ * by quarter, so the result can differ from tcp_mvp_apply_into_device in the
+ * last bits.
  */
 int tcp_mvp_apply_into_host(const tcp_mvp_plan *plan, const double *state, uint64_t state_len,
                             double *result, uint64_t result_len, uint64_t max_bytes);
