@@ -149,3 +149,28 @@ def test_plan_create_argument_errors() -> None:
         == _native.TCP_ERR_NON_FINITE_COEFFICIENT
     )
     assert lib.tcp_mvp_plan_create(2, 0, 1, None, None, None, 0, 0, None) == _native.TCP_ERR_INVALID_ARGUMENT
+
+
+def test_solver_kernel_limits_are_checked_before_any_launch() -> None:
+    """tcp_gram / tcp_block_combine reject shapes outside their launch limits
+    with InvalidArgument, and empty problems return at once; none of these
+    calls reaches the device."""
+    lib = _native.load_library()
+    dummy = ctypes.c_void_p(16)  # never dereferenced: every call below returns before a launch
+    c128, c64 = _native.TCP_DTYPE_C128, _native.TCP_DTYPE_C64
+    bad = _native.TCP_ERR_INVALID_ARGUMENT
+    # Gram: p + q <= 96, p * q <= 512, known storage types
+    assert lib.tcp_gram(dummy, c128, 90, dummy, c128, 7, 1024, dummy, dummy, None) == bad
+    assert "p + q <= 96" in _native.last_error()
+    assert lib.tcp_gram(dummy, c64, 40, dummy, c64, 13, 1024, dummy, dummy, None) == bad
+    assert lib.tcp_gram(dummy, 5, 4, dummy, c128, 4, 1024, dummy, dummy, None) == bad
+    assert lib.tcp_gram(dummy, c128, 0, dummy, c128, 4, 1024, dummy, dummy, None) == 0
+    assert lib.tcp_gram(None, c128, 4, dummy, c128, 4, 1024, dummy, dummy, None) == bad
+    # combine: up to 32 outputs, p x (outputs rounded up to 4, 8, 16 or 32) <= 6144
+    assert lib.tcp_block_combine(dummy, c128, 8, dummy, 33, 1024, 1.0, 0.0, dummy, c128, None) == bad
+    assert "k <= 32" in _native.last_error()
+    assert lib.tcp_block_combine(dummy, c64, 400, dummy, 17, 1024, 1.0, 0.0, dummy, c64, None) == bad
+    assert "coefficient block too large" in _native.last_error()
+    assert lib.tcp_block_combine(dummy, c64, 192, dummy, 17, 0, 1.0, 0.0, dummy, c64, None) == 0
+    assert lib.tcp_block_combine(dummy, c128, 8, dummy, 0, 1024, 1.0, 0.0, dummy, c128, None) == 0
+    assert lib.tcp_block_combine(None, c128, 8, dummy, 4, 1024, 1.0, 0.0, dummy, c128, None) == bad
