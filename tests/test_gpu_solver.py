@@ -69,6 +69,8 @@ def test_gram_and_combine_match_fp64_numpy(adt) -> None:
         (64, 4, torch.complex64, torch.complex64, 150002),  # register tiles, two rows per lane
         (52, 4, torch.complex128, torch.complex128, 100003),  # TMA: 13 tiles, several chunks per CTA, tail
         (13, 1, torch.complex128, torch.complex128, 65536),  # TMA: no tail
+        (10, 2, torch.complex128, torch.complex128, 50000),  # TMA: 8 x 2 tiles, ragged in p
+        (6, 3, torch.complex128, torch.complex128, 3000),  # TMA: q padded to 4, fewer rows than one chunk per CTA
         (20, 2, torch.complex64, torch.complex64, 70000),
     ],
 )
