@@ -20,6 +20,8 @@ constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
 constexpr uint32_t kCompensateGroups = 4;   // FP32: groups per Kahan fold
 
+constexpr uint32_t kPassBits = 2;            // host path: the state goes in as 4 parts
+constexpr uint32_t kPassChunks = 1u << kPassBits;
 constexpr uint32_t kNoPasses = 0xffffffffu;
 
 // Error bits written by kernels into the plan's device status word.
@@ -33,12 +35,12 @@ struct DevSchedule {
     uint32_t nsteps;
     uint32_t tile_bits;
     // Source-chunk passes of the host path: steps [pass_begin[v],
-    // pass_begin[v + 1]) have outer patterns d whose top two bits equal v
-    // (steps are sorted by d), so in pass k an output tile t reads only
-    // source tiles t ^ d in the quarter k of the state when v = k ^ (t >>
-    // pass_shift).  pass_shift = kNoPasses when the state has fewer than 4
-    // tiles.
-    uint32_t pass_begin[5];
+    // pass_begin[v + 1]) have outer patterns d whose top kPassBits bits equal
+    // v (steps are sorted by d), so in pass k an output tile t reads only
+    // source tiles t ^ d in the k-th of kPassChunks equal parts of the state
+    // when v = k ^ (t >> pass_shift).  pass_shift = kNoPasses when the state
+    // has fewer than kPassChunks tiles.
+    uint32_t pass_begin[kPassChunks + 1];
     uint32_t pass_shift;
     // group view (row kernel, transition count, diagonal): unfolded weights
     const uint64_t *g_mask;

@@ -137,8 +137,9 @@ __device__ __forceinline__ void issue_step(const uint4 info, uint64_t tile, cons
 // thread t owns rows t + j * kThreads of the tile.  Shared memory: two source
 // tiles and two step blocks (double buffering), refilled by the TMA engine.
 // PASSES = false runs every step and overwrites y.  PASSES = true runs pass
-// `pass` (0..3): only the steps whose source tiles lie in quarter `pass` of
-// the state (see DevSchedule::pass_begin), adding to y when `accumulate`.
+// `pass` (0..kPassChunks-1): only the steps whose source tiles lie in part
+// `pass` of the state (see DevSchedule::pass_begin), adding to y when
+// `accumulate`.
 template <int LOGE, typename R, bool PASSES>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tiled(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
@@ -159,11 +160,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     if constexpr (PASSES) {
         // constant indices only: a computed index into the parameter struct
         // would copy it to the stack
-        const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.pass_shift)) & 3u;
-        const uint32_t* pb = s.pass_begin;
-        step0 = v == 0u ? pb[0] : (v == 1u ? pb[1] : (v == 2u ? pb[2] : pb[3]));
-        const uint32_t step1 = v == 0u ? pb[1] : (v == 1u ? pb[2] : (v == 2u ? pb[3] : pb[4]));
-        nsteps = step1 - step0;
+        const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.pass_shift)) & (kPassChunks - 1u);
+        uint32_t b0 = s.pass_begin[0], b1 = s.pass_begin[1];
+#pragma unroll
+        for (uint32_t w = 1; w < kPassChunks; ++w) {
+            if (v == w) {
+                b0 = s.pass_begin[w];
+                b1 = s.pass_begin[w + 1];
+            }
+        }
+        step0 = b0;
+        nsteps = b1 - b0;
     }
     const uint4 *steps = s.step_info + step0;
     const unsigned char *blocks = step_blocks<R>(s);
@@ -337,28 +344,32 @@ using tcp::overlaps;
 namespace {
 
 int g_num_sms = 0;
-constexpr uint64_t kHostChunks = 8;  // output-tile chunks of a large host apply
+// Host apply at n = 28 (65,536 tiles): 4 input parts and 8 output chunks
+// measured 280 ms; 8 parts and 16 chunks measured 312 ms (more passes over
+// y and more pass start-up than the shorter exposed copies save).
+constexpr uint64_t kHostChunks = 8;         // output-tile chunks of a large host apply
+constexpr uint64_t kHostChunkTiles = 8192;  // tiles from which the host apply is chunked
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Step ranges of the source-chunk passes (see DevSchedule::pass_begin): the
-// top two bits v of each step's outer pattern d, which is non-decreasing in
-// step order because steps are sorted by d.
+// top kPassBits bits v of each step's outer pattern d, which is
+// non-decreasing in step order because steps are sorted by d.
 void set_passes(DevSchedule &dev, const tcp::Schedule &h, uint32_t nqubits) {
     const uint32_t nsteps = static_cast<uint32_t>(h.step_info.size() / 4);
     dev.pass_shift = kNoPasses;
-    for (int v = 0; v < 5; ++v) dev.pass_begin[v] = v == 0 ? 0u : nsteps;
-    if (nqubits < h.tile_bits + 2) return;
-    const uint32_t shift = nqubits - h.tile_bits - 2;
+    for (uint32_t v = 0; v <= kPassChunks; ++v) dev.pass_begin[v] = v == 0 ? 0u : nsteps;
+    if (nqubits < h.tile_bits + kPassBits) return;
+    const uint32_t shift = nqubits - h.tile_bits - kPassBits;
     uint32_t prev = 0;
     for (uint32_t st = 0; st < nsteps; ++st) {
         const uint64_t d = static_cast<uint64_t>(h.step_info[4 * st]) | (static_cast<uint64_t>(h.step_info[4 * st + 1]) << 32);
         const uint32_t v = static_cast<uint32_t>(d >> shift);
-        if (v > 3 || v < prev) return;  // not a sorted schedule: no passes
+        if (v >= kPassChunks || v < prev) return;  // not a sorted schedule: no passes
         for (uint32_t w = prev + 1; w <= v; ++w) dev.pass_begin[w] = st;
         prev = v;
     }
-    for (uint32_t w = prev + 1; w <= 4; ++w) dev.pass_begin[w] = nsteps;
+    for (uint32_t w = prev + 1; w <= kPassChunks; ++w) dev.pass_begin[w] = nsteps;
     dev.pass_shift = shift;
 }
 
@@ -535,35 +546,35 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     int status = TCP_OK;
     if (e != cudaSuccess) status = cuda_fail(e, "cudaStreamCreate");
     // Large tiled applies overlap both copies with the kernel.
-    //  * Input: the state goes in as four quarters on its own stream.  Pass k
-    //    (k = 0..3) waits for quarter k only and runs the steps whose source
+    //  * Input: the state goes in as kPassChunks equal parts on its own
+    //    stream.  Pass k waits for part k only and runs the steps whose source
     //    tiles lie in it (k_tiled's `pass`), adding to y after the first, so
-    //    the copy of quarters 1..3 overlaps passes 0..2.
+    //    the copy of parts 1.. overlaps the earlier passes.
     //  * Output: the last pass runs in kHostChunks launches over consecutive
     //    output tiles; a third stream copies each finished chunk of y to the
     //    host while the next chunk computes.
     // All copies and launches are queued before the host waits on any of
     // them.  Smaller applies copy, launch once and copy back on one stream.
     const uint64_t tiles = tiled_tiles<R>(plan, ws.x);
-    const uint64_t chunks = tiles >= kHostChunks * 1024 ? kHostChunks : 1;
+    const uint64_t chunks = tiles >= kHostChunkTiles ? kHostChunks : 1;
     const bool passes = chunks > 1 && plan->sched.dev.pass_shift != kNoPasses;
-    constexpr int kQuarters = 4;
+    constexpr int kParts = static_cast<int>(kPassChunks);
     cudaStream_t copy_stream = nullptr, in_stream = nullptr;
     cudaEvent_t done[kHostChunks] = {};
-    cudaEvent_t landed[kQuarters] = {};
+    cudaEvent_t landed[kParts] = {};
     if (!status && chunks > 1) {
         e = cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking);
         for (uint64_t c = 0; c < chunks && e == cudaSuccess; ++c) e = cudaEventCreateWithFlags(&done[c], cudaEventDisableTiming);
         if (passes && e == cudaSuccess) e = cudaStreamCreateWithFlags(&in_stream, cudaStreamNonBlocking);
-        for (int k = 0; passes && k < kQuarters && e == cudaSuccess; ++k)
+        for (int k = 0; passes && k < kParts && e == cudaSuccess; ++k)
             e = cudaEventCreateWithFlags(&landed[k], cudaEventDisableTiming);
         if (e != cudaSuccess) status = cuda_fail(e, "creating the copy streams");
     }
     if (!status && passes) {
-        const size_t quarter = bytes / kQuarters;
-        for (int k = 0; k < kQuarters && !status; ++k) {
-            e = cudaMemcpyAsync(static_cast<unsigned char *>(ws.x) + k * quarter,
-                                reinterpret_cast<const unsigned char *>(state) + k * quarter, quarter,
+        const size_t part = bytes / kParts;
+        for (int k = 0; k < kParts && !status; ++k) {
+            e = cudaMemcpyAsync(static_cast<unsigned char *>(ws.x) + k * part,
+                                reinterpret_cast<const unsigned char *>(state) + k * part, part,
                                 cudaMemcpyHostToDevice, in_stream);
             if (e == cudaSuccess) e = cudaEventRecord(landed[k], in_stream);
             if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
@@ -573,19 +584,19 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
     }
     if (!status && chunks > 1) {
-        for (int k = 0; passes && k < kQuarters - 1 && !status; ++k) {
+        for (int k = 0; passes && k < kParts - 1 && !status; ++k) {
             e = cudaStreamWaitEvent(stream, landed[k], 0);
-            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input quarter");
+            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
             if (!status) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
         }
         if (!status && passes) {
-            e = cudaStreamWaitEvent(stream, landed[kQuarters - 1], 0);
-            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input quarter");
+            e = cudaStreamWaitEvent(stream, landed[kParts - 1], 0);
+            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
         }
         const uint64_t per = tiles / chunks;
         for (uint64_t c = 0; c < chunks && !status; ++c) {
             const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
-            status = passes ? launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, kQuarters - 1, true)
+            status = passes ? launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, kParts - 1, true)
                             : launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
             if (!status) {
                 e = cudaEventRecord(done[c], stream);
