@@ -66,6 +66,41 @@ def _profile_traffic(kernel: str) -> Optional[float]:
     return None
 
 
+def manifest(with_gpu: bool = True) -> Dict[str, Any]:
+    """What produced a bench line: the library's build record (source commit,
+    nvcc release), a digest of the sources as they ran, host core count,
+    driver, toolkit and framework versions."""
+    import hashlib
+    import platform
+
+    info: Dict[str, Any] = {"nproc": os.cpu_count(), "python": platform.python_version(), "numpy": np.__version__}
+    build_info = os.path.join(ROOT, "tencirpauli_b200", "_lib", "build_info.json")
+    if os.path.exists(build_info):
+        with open(build_info) as fh:
+            info["build"] = json.load(fh)
+    digest = hashlib.sha256()
+    csrc = os.path.join(ROOT, "tencirpauli_b200", "csrc")
+    for name in sorted(os.listdir(csrc)) + ["../../bench.py"]:
+        with open(os.path.join(csrc, name), "rb") as fh:
+            digest.update(fh.read())
+    info["sources_sha16"] = digest.hexdigest()[:16]
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=driver_version,name", "--format=csv,noheader"],
+                             capture_output=True, text=True, timeout=20).stdout.strip().splitlines()
+        if out:
+            driver, name = (p.strip() for p in out[0].split(",", 1))
+            info["driver"] = driver
+            info["gpu"] = name
+    except (OSError, subprocess.SubprocessError, ValueError):
+        pass
+    if with_gpu:
+        import torch
+
+        info["torch"] = torch.__version__
+        info["torch_cuda"] = torch.version.cuda
+    return info
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -189,28 +224,71 @@ def cpu_reference_rate(op, state_host: np.ndarray, seconds: float, threads: int 
     }
 
 
+def _standalone_workloads():
+    """``tencirpauli_b200/workloads.py`` loaded on its own (pure NumPy), so that
+    the reference arm never imports the product package or maps its library."""
+    import importlib.util
+
+    path = os.path.join(ROOT, "tencirpauli_b200", "workloads.py")
+    spec = importlib.util.spec_from_file_location("_tcp_bench_workloads", path)
+    module = importlib.util.module_from_spec(spec)
+    assert spec.loader is not None
+    spec.loader.exec_module(module)
+    return module
+
+
 def run_reference(args: argparse.Namespace) -> None:
+    """The reference's CPU algorithm on this host's cores: the C restatement
+    of the Rust/rayon TermDirect row loop (crates/tencir-pauli-core/src/
+    hamiltonian.rs:204-270; the Rust build is unavailable), on the same
+    canonical operator and state as the GPU arm.  A step is the row loop over
+    one block of ``2^reference_rows_log2`` consecutive rows (blocks walk the
+    state in order), so ``ms_per_step`` x ``steps`` is the time this arm ran.
+    The canonical term list comes from the oracle's restatement of
+    PauliOperator::from_terms (operator.rs:117-155): nothing of the product
+    is imported.  After the timed steps, one full TermDirect pass over the
+    whole state is timed once and reported as ``full_pass_s``."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle
 
-    op = build_operator(args)
-    n = op.nqubits
+    wl = _standalone_workloads()
+    n = args.nqubits
+    codes, coeffs = wl.random_k_local(n=n, words=args.words, seed=args.seed)
+    xw, zw, cf = oracle.canonicalize(n, codes, coeffs)
+    xm, zm, wp = oracle.matrix_terms(n, xw, zw, cf)
+    T = len(cf)
+    dim = 1 << n
     rng = np.random.default_rng(args.seed)
-    state = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    state = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
     state /= np.linalg.norm(state)
     cores = oracle.max_threads()
-    for _ in range(args.warmup):
-        cpu_reference_rate(op, state, seconds=0.5, threads=cores)
-    rates = []
-    samples = []
-    for _ in range(args.steps):
-        r = cpu_reference_rate(op, state, seconds=args.reference_seconds, threads=cores)
-        rates.append(r["value"])
-        samples.append(r)
-    value = float(statistics.median(rates))
-    amp_terms_per_step = op.term_count * (1 << n)
+    rows_per_step = min(dim, 1 << args.reference_rows_log2)
+    blocks = dim // rows_per_step
+    block_rows = np.arange(rows_per_step, dtype=np.uint64)
+
+    def step(i: int) -> float:
+        rows = block_rows + np.uint64((i % blocks) * rows_per_step)
+        t0 = time.perf_counter()
+        oracle.apply_rows(n, xm, zm, wp, state, rows, cores)
+        return time.perf_counter() - t0
+
+    for i in range(args.warmup):
+        step(i)
+    times = [step(args.warmup + i) for i in range(args.steps)]
+    seconds = float(sum(times))
+    value = T * rows_per_step * args.steps / seconds
+    full_pass_s = None
+    if args.reference_full_pass:
+        t0 = time.perf_counter()
+        oracle.apply_term_direct(n, xm, zm, wp, state, cores)
+        full_pass_s = time.perf_counter() - t0
+    config = workload_config(args, None, terms=T)
+    config["rows_per_step"] = rows_per_step
+    sample = (f"{args.steps} blocks of {rows_per_step} consecutive rows of the 2^{n} state x {T} terms "
+              f"(TermDirect row loop, {seconds:.1f} s); C restatement of the reference Rust MVP "
+              "(Rust build unavailable)")
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -219,36 +297,40 @@ def run_reference(args: argparse.Namespace) -> None:
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1000.0 * amp_terms_per_step / value,
+        "ms_per_step": 1000.0 * seconds / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": workload_config(args, op),
-        "cpu_baseline": {
-            "value": value,
-            "unit": UNIT,
-            "cores": cores,
-            "kind": "port",
-            "sample": samples[-1]["sample"] + "; C restatement of the reference Rust MVP (Rust build unavailable)",
-        },
+        "config": config,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "full_pass_s": full_pass_s,
+        "full_pass_amp_terms_per_s": (T * dim / full_pass_s) if full_pass_s else None,
+        "manifest": manifest(with_gpu=False),
     }
     print(json.dumps(line), flush=True)
 
 
-def workload_config(args: argparse.Namespace, op) -> Dict[str, Any]:
+def workload_config(args: argparse.Namespace, op, terms: Optional[int] = None) -> Dict[str, Any]:
     return {
         "workload": f"random {args.words}-word 2..4-local Hamiltonian, n={args.nqubits}",
         "nqubits": args.nqubits,
         "raw_words": args.words,
-        "terms": op.term_count,
+        "terms": op.term_count if op is not None else terms,
         "seed": args.seed,
         "state": "complex128" if args.dtype == "c128" else "complex64",
         "vectors_per_step_per_gpu": 1,
-        "l2": "inputs larger than L2 (4 GiB per vector), no flush",
+        "l2": _l2_note(args.nqubits, 16 if args.dtype == "c128" else 8),
     }
+
+
+def _l2_note(n: int, elem: int) -> str:
+    vec = (1 << n) * elem
+    if vec > 126 * 2**20:
+        return f"inputs larger than L2 ({vec / 2**30:.2f} GiB per vector), no flush"
+    return f"vector of {vec / 2**20:.1f} MiB fits in L2 (not flushed between steps)"
 
 
 def run_batched(args: argparse.Namespace) -> None:
@@ -672,7 +754,10 @@ def main() -> None:
     parser.add_argument("--dtype", choices=["c128", "c64"], default="c128")
     parser.add_argument("--e2e-steps", type=int, default=3)
     parser.add_argument("--cpu-seconds", type=float, default=15.0)
-    parser.add_argument("--reference-seconds", type=float, default=10.0)
+    parser.add_argument("--reference-rows-log2", type=int, default=22,
+                        help="reference arm: rows per step (log2) of the TermDirect row loop")
+    parser.add_argument("--reference-full-pass", type=int, default=1,
+                        help="reference arm: also time one full pass over the state (1) or not (0)")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -850,6 +935,7 @@ def main() -> None:
             },
             "gpu_launches": args.steps,
             "clocks": clocks,
+            "manifest": manifest(),
             "plan": {
                 "groups": plan.group_count,
                 "tile_bits": int(native.info.tile_bits),

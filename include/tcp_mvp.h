@@ -63,6 +63,21 @@ enum tcp_dtype {
     TCP_DTYPE_C64 = 1   /* complex64 state, FP32 products, Kahan sum over groups */
 };
 
+/* The calling thread's last status and the numeric fields of its PauliError
+ * variant, so that a binding can rebuild the variant without parsing the
+ * message of tcp_last_error (crates/tencir-pauli-core/src/error.rs:5-74):
+ *   TCP_ERR_INVALID_CODE             fields = {code, index}
+ *   TCP_ERR_INVALID_WORD_LENGTH,
+ *   TCP_ERR_INVALID_STRUCTURE_LENGTH fields = {expected, actual}
+ *   TCP_ERR_NON_FINITE_COEFFICIENT   fields = {index, 0}
+ *   TCP_ERR_MEMORY_LIMIT             fields = {requested, limit} (requested
+ *                                    saturates at 2^64 - 1)
+ *   TCP_ERR_SECTOR_LEAKAGE (11)      fields = {source_index, actual}; the
+ *                                    expected weight is the sector's k
+ * Other statuses carry no fields (both 0).  Returns the last status (0 when
+ * the thread has had no error). */
+int tcp_last_error_fields(uint64_t fields[2]);
+
 /* Opaque, immutable-after-create plan.  Thread-safe for concurrent apply. */
 typedef struct tcp_mvp_plan tcp_mvp_plan;
 
@@ -140,7 +155,8 @@ int tcp_mvp_plan_info(const tcp_mvp_plan *plan, tcp_mvp_plan_info_t *info);
  * in chunks of output tiles while later chunks compute; page-locked host
  * buffers let the copies overlap the kernel.  The FP64 sums are then grouped
  * by quarter, so the result can differ from tcp_mvp_apply_into_device in the
- * last bits.
+ * last bits.  After TCP_ERR_DEVICE_TIMEOUT the contents of `result` are
+ * undefined.
  */
 int tcp_mvp_apply_into_host(const tcp_mvp_plan *plan, const double *state, uint64_t state_len,
                             double *result, uint64_t result_len, uint64_t max_bytes);
@@ -211,6 +227,7 @@ int tcp_mvp_batch_device_status(tcp_mvp_batch *batch);
  *  - Runs on `stream` (a cudaStream_t, NULL for the legacy default stream) and
  *    returns after the result is in `result`.  Semantics otherwise equal
  *    tcp_mvp_apply_into_host (lengths, overwrite, errors).
+ *  - When it returns TCP_ERR_DEVICE_TIMEOUT, `result` has been set to zero.
  */
 #define TCP_NOALLOC_MAX_QUBITS 20
 int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const double *state,

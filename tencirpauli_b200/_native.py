@@ -50,6 +50,7 @@ U64_MAX = (1 << 64) - 1
 EXPORTED_SYMBOLS = (
     "tcp_abi_version",
     "tcp_last_error",
+    "tcp_last_error_fields",
     "tcp_pauli_canonicalize",
     "tcp_mvp_plan_create",
     "tcp_mvp_plan_destroy",
@@ -178,6 +179,8 @@ def load_library() -> ctypes.CDLL:
         u32, u64, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
         lib.tcp_abi_version.restype = i32
         lib.tcp_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        lib.tcp_last_error_fields.argtypes = [u64p]
+        lib.tcp_last_error_fields.restype = i32
         lib.tcp_last_error.restype = ctypes.c_size_t
         lib.tcp_pauli_canonicalize.argtypes = [u32, u64, u8p, f64p, u64p, u64p, f64p, u64p, u64p]
         lib.tcp_mvp_plan_create.argtypes = [u32, u64, u32, u64p, u64p, f64p, i32, u64, ctypes.POINTER(vp)]
@@ -251,6 +254,15 @@ def last_error() -> str:
     buf = ctypes.create_string_buffer(1024)
     lib.tcp_last_error(buf, len(buf))
     return buf.value.decode("utf-8", "replace")
+
+
+def last_error_fields() -> Tuple[int, int, int]:
+    """(status, field 0, field 1) of this thread's last error: the numeric
+    fields of the matching PauliError variant (see tcp_last_error_fields)."""
+    lib = load_library()
+    fields = (ctypes.c_uint64 * 2)()
+    status = lib.tcp_last_error_fields(fields)
+    return int(status), int(fields[0]), int(fields[1])
 
 
 class NativeDeviceError(RuntimeError):

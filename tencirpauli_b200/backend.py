@@ -25,6 +25,11 @@ from ._native_mvp import DEFAULT_MAX_BYTES, check_allocation, validate_max_bytes
 _FACTORY = object()
 
 
+def _is_capsule(value: Any) -> bool:
+    """A bare DLPack capsule (``PyCapsule`` named "dltensor")."""
+    return type(value).__name__ == "PyCapsule"
+
+
 @dataclass(frozen=True)
 class BackendMVPPlan:
     schema_version: int
@@ -97,6 +102,8 @@ class BackendMVPPlan:
         """H @ state.  NumPy input -> NumPy complex128 output (host copies);
         a device array -> a device array of the same dtype, no host copy."""
         validate_max_bytes(max_bytes)
+        if _is_capsule(state):
+            return self.device_callable()(state)
         if isinstance(state, np.ndarray) or not hasattr(state, "__dlpack__"):
             values = np.ascontiguousarray(np.asarray(state, dtype=np.complex128))
             if values.shape != (self.dimension,):
@@ -109,13 +116,19 @@ class BackendMVPPlan:
 
     def device_callable(self):
         """f(x) -> H x for device arrays (complex128 or complex64, shape (2^n,)
-        or (k, 2^n)) from any DLPack producer; returns a torch CUDA tensor."""
+        or (k, 2^n)) from any DLPack producer -- an object with ``__dlpack__``
+        or a bare DLPack capsule; returns a torch CUDA tensor."""
         import torch
 
         plan = self._plan()
 
         def apply(x: Any) -> Any:
-            t = x if isinstance(x, torch.Tensor) else torch.from_dlpack(x)
+            if isinstance(x, torch.Tensor):
+                t = x
+            elif _is_capsule(x):
+                t = torch.utils.dlpack.from_dlpack(x)
+            else:
+                t = torch.from_dlpack(x)
             if t.device.type != "cuda":
                 raise ValueError("device_callable needs a device array")
             t = t.contiguous()

@@ -61,7 +61,36 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
     if ptxas_verbose or verbose:
         sys.stdout.write(proc.stdout + proc.stderr)
     os.replace(LIBPATH + ".tmp", LIBPATH)
+    _write_build_info()
     return LIBPATH
+
+
+def _git(*args: str) -> str:
+    try:
+        proc = subprocess.run(["git", *args], cwd=os.path.dirname(HERE), capture_output=True, text=True, timeout=30)
+        return proc.stdout.strip() if proc.returncode == 0 else ""
+    except (OSError, subprocess.SubprocessError):
+        return ""
+
+
+def _write_build_info() -> None:
+    """Record what the library was built from (``_lib/build_info.json``): the
+    source commit (and whether the tree had local changes), the nvcc release
+    and the target architecture.  Benchmark lines carry it as their manifest."""
+    import json
+
+    try:
+        release = subprocess.run([nvcc(), "--version"], capture_output=True, text=True).stdout.strip().splitlines()[-1]
+    except (OSError, IndexError):
+        release = ""
+    info = {
+        "commit": _git("rev-parse", "HEAD"),
+        "dirty": bool(_git("status", "--porcelain", "--", "tencirpauli_b200", "include")),
+        "nvcc": release,
+        "arch": "sm_100a",
+    }
+    with open(os.path.join(LIBDIR, "build_info.json"), "w") as fh:
+        json.dump(info, fh)
 
 
 if __name__ == "__main__":

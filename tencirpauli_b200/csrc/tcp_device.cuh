@@ -42,6 +42,14 @@ struct DevSchedule {
     // has fewer than kPassChunks tiles.
     uint32_t pass_begin[kPassChunks + 1];
     uint32_t pass_shift;
+    // ring view (k_ring; see tcp::RingSchedule): ring_steps = 0 when the
+    // plan has no ring schedule.  Pass ranges as above, over the ring steps.
+    const uint4 *ring_info;          // d lo, d hi, block offset / 16, block bytes / 16
+    const unsigned char *ring128;    // blocks with FP64 weights
+    const unsigned char *ring64;     // blocks with FP32 weights
+    uint32_t ring_steps;
+    uint32_t ring_pass_begin[kPassChunks + 1];
+    uint32_t ring_pass_shift;
     // group view (row kernel, transition count, diagonal): unfolded weights
     const uint64_t *g_mask;
     const uint32_t *g_tbeg;
@@ -77,6 +85,10 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
+// Plain arrive (count 1) on an mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ uint32_t mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -99,6 +111,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     for (uint32_t spin = 1;; ++spin) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((spin & 255u) == 0u && global_ns() - start > limit_ns) return false;
+    }
+}
+
+// Bounded wait that also gives up as soon as another thread of the CTA has
+// raised `abort_flag` (a shared-memory word); returns false on either.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parity, const volatile int *abort_flag,
+                                                   unsigned long long limit_ns = kWaitLimitNs) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long start = global_ns();
+    for (uint32_t spin = 1;; ++spin) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((spin & 63u) == 0u && (*abort_flag || global_ns() - start > limit_ns)) return false;
     }
 }
 

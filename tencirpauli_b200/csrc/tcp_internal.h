@@ -15,6 +15,13 @@ namespace tcp {
 // Thread-local last-error slot behind tcp_last_error().
 void set_error(const std::string &message);
 int fail(int status, const std::string &message);
+// The same with the numeric fields of the PauliError variant (expected /
+// actual, requested / limit, code / index, index / 0), read back through
+// tcp_last_error_fields so that a binding can rebuild the variant exactly.
+int fail_fields(int status, const std::string &message, uint64_t a, uint64_t b);
+uint64_t clamp_u64(unsigned __int128 v);
+// InvalidStructureLength {expected, actual}: "expected structure length E, got A"
+int length_error(uint64_t expected, uint64_t actual);
 
 // One compiled term: StatevectorPauliAction masks in the MSB index space and
 // the weighted phase c * i^{#Y} (pauli_action.rs:58-86, hamiltonian.rs:564-571).
@@ -66,6 +73,40 @@ struct Schedule {
     std::vector<double> t_w;          // weighted phase (re, im), schedule order
     std::vector<float> t_wf;          // the same rounded to FP32 (re, im)
 };
+
+// Schedule of the ring kernel (k_ring).  Same tiles and steps as Schedule
+// (one step per distinct outer pattern d, split when its block outgrows
+// kRingBlockBytes), but the groups of a step are arranged in cosets: groups
+// whose inner masks agree on the thread bits (m & (2^log_threads - 1)) read
+// the same 2^(S - log_threads) source values per thread, in a permuted order,
+// so the values are loaded once per coset and every group of the coset
+// applies them through a compile-time register permutation a = jh ^ jh_load.
+// Block layout (16-byte units):
+//   header    {ncosets, ngroups, terms offset / 16, 0}
+//   cosets    {m_lo, jh_load, groups in the coset, 0} each
+//   groups    u32 each: a | nterms << 4, padded to 16 bytes
+//   terms     16 bytes each: meta = zlo | pattern << 9 | imag << 17, zt32 =
+//             z >> S (low 32 bits), then the folded weight: one f64
+//             (complex128 blocks) or one f32 + 4 pad bytes (complex64 blocks).
+// A weight is real (imag = 0) or imaginary (imag = 1); a term with a complex
+// weight is stored as two records with the same z.  The folded sign is
+// parity(zt & d) ^ parity(zlo & m_lo) ^ parity(zj & jh) as in Schedule, so the
+// remaining sign of row j is parity(zlo & t) ^ parity(zt & tile) ^ bit j of
+// the pattern.  Needs n - S <= 32 (zt32 holds every outer z bit).
+struct RingSchedule {
+    uint32_t tile_bits = 0;
+    uint32_t log_threads = 0;
+    uint64_t cosets = 0;               // coset loads per output tile
+    uint32_t max_block_bytes = 0;      // largest step block
+    std::vector<uint32_t> step_info;   // d lo, d hi, block offset / 16, block bytes / 16
+    std::vector<uint8_t> blocks_c128;
+    std::vector<uint8_t> blocks_c64;
+};
+
+constexpr uint32_t kRingBlockBytes = 8192;
+
+RingSchedule build_ring_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits,
+                                 uint32_t log_threads);
 
 constexpr uint32_t kBlockBytesMax = 16384;
 constexpr uint32_t kGroupRecBytes = 16;

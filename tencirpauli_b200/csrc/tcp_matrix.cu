@@ -90,8 +90,9 @@ std::string bytes_text(unsigned __int128 v) {
 }
 
 int memory_limit(unsigned __int128 requested, uint64_t limit) {
-    return fail(TCP_ERR_MEMORY_LIMIT, "requested " + bytes_text(requested) + " bytes exceeds memory limit " +
-                                          std::to_string(limit));
+    return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                            "requested " + bytes_text(requested) + " bytes exceeds memory limit " + std::to_string(limit),
+                            tcp::clamp_u64(requested), limit);
 }
 
 // The reference's budget for a sparse target (hamiltonian.rs:358-445):

@@ -231,6 +231,233 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ------------------------------- ring kernel --------------------------------
+// k_ring: the tiled MVP with a warp-specialised ring of source tiles.
+//  * One producer warp (its lane 0) streams the steps of the output tile: it
+//    waits until the consumers have released a stage ("empty" mbarrier), then
+//    has the TMA bulk-copy engine fill that stage with the step's source tile
+//    (tile ^ d) and its block ("full" mbarrier with the byte count).
+//  * Sixteen consumer warps own the tile's 4096 rows (thread t: rows
+//    t + j * 512, j = 0..7) and keep their sums in registers.  Per step they
+//    wait for the stage, walk its cosets -- one row-ordered load of 8 source
+//    values per coset -- and apply every group of the coset through a
+//    compile-time register permutation a (row j reads loaded value j ^ a).
+//    Then each warp releases the stage with one arrive.  No CTA-wide barrier
+//    runs after set-up, so warps drift apart by up to the ring depth.
+//  * Every wait is bounded (2 s) and also ends when another thread raised the
+//    CTA's abort word; the kernel then records kErrTimeout.  The producer
+//    always waits (bounded) for the last copy it issued into each stage before
+//    it exits, so no copy is left writing into a finished block's memory.
+constexpr int kRingConsumerWarps = kThreads / 32;
+constexpr int kRingThreads = kThreads + 32;
+
+template <typename R> struct RingDepth;
+template <> struct RingDepth<double> { static constexpr uint32_t K = 3; };  // 3 x (64 + 8) KiB
+template <> struct RingDepth<float> { static constexpr uint32_t K = 5; };   // 5 x (32 + 8) KiB
+
+template <typename R> constexpr uint32_t ring_tile_bytes() {
+    return (1u << kTileBitsC128) * static_cast<uint32_t>(sizeof(typename Cx<R>::T));
+}
+template <typename R> constexpr uint32_t ring_stage_bytes() { return ring_tile_bytes<R>() + tcp::kRingBlockBytes; }
+template <typename R> constexpr size_t ring_smem_bytes() {
+    return static_cast<size_t>(RingDepth<R>::K) * ring_stage_bytes<R>();
+}
+
+template <typename R> __device__ __forceinline__ const unsigned char *ring_blocks(const DevSchedule &s);
+template <> __device__ __forceinline__ const unsigned char *ring_blocks<double>(const DevSchedule &s) {
+    return s.ring128;
+}
+template <> __device__ __forceinline__ const unsigned char *ring_blocks<float>(const DevSchedule &s) {
+    return s.ring64;
+}
+
+// Weight of a ring term record: one f64 (bytes 8..15) or one f32 (bytes 8..11).
+template <typename R> __device__ __forceinline__ R ring_weight(uint4 rec);
+template <> __device__ __forceinline__ double ring_weight<double>(uint4 rec) {
+    return __hiloint2double(static_cast<int>(rec.w), static_cast<int>(rec.z));
+}
+template <> __device__ __forceinline__ float ring_weight<float>(uint4 rec) { return __uint_as_float(rec.z); }
+
+// One term record applied to the thread's 8 rows, row j reading loaded value
+// j ^ A.  Sign of row j: parity(zlo & t) ^ parity(zt & tile) ^ bit j of the
+// pattern (the rest is folded into the weight).  meta & t keeps only the zlo
+// bits because t < 512.
+template <int A, typename R>
+__device__ __forceinline__ void ring_term(uint4 rec, uint32_t tid, uint32_t tile32,
+                                          const typename Cx<R>::T (&xv)[8], Acc<R> (&acc)[8]) {
+    const uint32_t meta = rec.x;
+    const uint32_t base = __popc((meta & tid) ^ (rec.y & tile32)) & 1u;
+    const uint32_t pattern = (meta >> 9) & 0xffu;
+    const bool imag = ((meta >> 17) & 1u) != 0u;
+    const R w = ring_weight<R>(rec);
+    if (pattern == 0u) {
+        const R ws = flip_by(w, base);
+        if (!imag) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j].add_real(ws, xv[j ^ A]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j].add_imag(ws, xv[j ^ A]);
+        }
+    } else {
+        const uint32_t pat = (pattern ^ (0u - base)) & 0xffu;
+        if (!imag) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j].add_real(flip_if(w, pat, j), xv[j ^ A]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j].add_imag(flip_if(w, pat, j), xv[j ^ A]);
+        }
+    }
+}
+
+template <int A, typename R>
+__device__ __forceinline__ void ring_group(const uint4 *__restrict__ trm, uint32_t nt, uint32_t tid, uint32_t tile32,
+                                           const typename Cx<R>::T (&xv)[8], Acc<R> (&acc)[8]) {
+    for (uint32_t k = 0; k < nt; ++k) ring_term<A, R>(trm[k], tid, tile32, xv, acc);
+}
+
+template <typename R, bool PASSES>
+__global__ void __launch_bounds__(kRingThreads, 1)
+    k_ring(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
+           int *__restrict__ err, uint64_t tile0, uint32_t pass, uint32_t accumulate) {
+    using C = typename Cx<R>::T;
+    constexpr uint32_t K = RingDepth<R>::K;
+    constexpr uint32_t TILE_BYTES = ring_tile_bytes<R>();
+    constexpr uint32_t STAGE = ring_stage_bytes<R>();
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[K];
+    __shared__ __align__(8) uint64_t empty[K];
+    __shared__ int abort_word;
+
+    const uint32_t tid = threadIdx.x;
+    const uint64_t tile = tile0 + blockIdx.x;
+    uint32_t step0 = 0, nsteps = s.ring_steps;
+    if constexpr (PASSES) {
+        const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.ring_pass_shift)) & (kPassChunks - 1u);
+        uint32_t b0 = s.ring_pass_begin[0], b1 = s.ring_pass_begin[1];
+#pragma unroll
+        for (uint32_t w = 1; w < kPassChunks; ++w) {
+            if (v == w) {
+                b0 = s.ring_pass_begin[w];
+                b1 = s.ring_pass_begin[w + 1];
+            }
+        }
+        step0 = b0;
+        nsteps = b1 - b0;
+    }
+    if (tid == 0) {
+#pragma unroll
+        for (uint32_t k = 0; k < K; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], kRingConsumerWarps);
+        }
+        abort_word = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+    volatile int *abort_flag = &abort_word;
+
+    if (tid >= static_cast<uint32_t>(kThreads)) {
+        // ---------------- producer warp (lane 0 issues) ----------------
+        if (tid != static_cast<uint32_t>(kThreads)) return;
+        const uint4 *info = s.ring_info + step0;
+        const unsigned char *blocks = ring_blocks<R>(s);
+        uint32_t issued = 0;
+        for (uint32_t st = 0; st < nsteps; ++st) {
+            const uint32_t stage = st % K;
+            if (st >= K && !mbar_wait_or_abort(&empty[stage], ((st / K) - 1u) & 1u, abort_flag)) {
+                atomicOr(err, kErrTimeout);
+                *abort_flag = 1;
+                break;
+            }
+            const uint4 in = __ldg(&info[st]);
+            const uint64_t d = static_cast<uint64_t>(in.x) | (static_cast<uint64_t>(in.y) << 32);
+            const uint32_t blk_bytes = in.w * 16u;
+            unsigned char *dst = smem_raw + stage * STAGE;
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&full[stage], TILE_BYTES + blk_bytes);
+            bulk_copy_g2s(dst, x + ((tile ^ d) << kTileBitsC128), TILE_BYTES, &full[stage]);
+            bulk_copy_g2s(dst + TILE_BYTES, blocks + static_cast<size_t>(in.z) * 16u, blk_bytes, &full[stage]);
+            issued = st + 1;
+        }
+        // the last copy issued into each stage has landed before this returns
+        for (uint32_t st = issued > K ? issued - K : 0u; st < issued; ++st) mbar_wait_bounded(&full[st % K], (st / K) & 1u);
+        return;
+    }
+
+    // ---------------- consumer warps ----------------
+    const uint32_t tile32 = static_cast<uint32_t>(tile);
+    Acc<R> acc[8];
+    uint32_t stage = 0, phase = 0;
+    for (uint32_t st = 0; st < nsteps; ++st) {
+        const bool landed = mbar_wait_or_abort(&full[stage], phase, abort_flag);
+        if (__any_sync(0xffffffffu, !landed)) {
+            if ((tid & 31u) == 0u) {
+                atomicOr(err, kErrTimeout);
+                *abort_flag = 1;
+            }
+            return;
+        }
+        const C *xs = reinterpret_cast<const C *>(smem_raw + stage * STAGE);
+        const unsigned char *blk = smem_raw + stage * STAGE + TILE_BYTES;
+        const uint4 hdr = *reinterpret_cast<const uint4 *>(blk);
+        const uint4 *cos = reinterpret_cast<const uint4 *>(blk + 16);
+        const uint32_t *gw = reinterpret_cast<const uint32_t *>(blk + 16u + hdr.x * 16u);
+        const uint4 *trm = reinterpret_cast<const uint4 *>(blk + hdr.z * 16u);
+        uint32_t g = 0;
+        for (uint32_t c = 0; c < hdr.x; ++c) {
+            const uint4 cr = cos[c];
+            C xv[8];
+            const C *src = xs + (tid ^ cr.x);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) xv[j] = src[(static_cast<uint32_t>(j) ^ cr.y) << kLogThreads];
+            for (uint32_t k = 0; k < cr.z; ++k, ++g) {
+                const uint32_t word = gw[g];
+                const uint32_t nt = word >> 4;
+                switch (word & 7u) {
+                case 0: ring_group<0, R>(trm, nt, tid, tile32, xv, acc); break;
+                case 1: ring_group<1, R>(trm, nt, tid, tile32, xv, acc); break;
+                case 2: ring_group<2, R>(trm, nt, tid, tile32, xv, acc); break;
+                case 3: ring_group<3, R>(trm, nt, tid, tile32, xv, acc); break;
+                case 4: ring_group<4, R>(trm, nt, tid, tile32, xv, acc); break;
+                case 5: ring_group<5, R>(trm, nt, tid, tile32, xv, acc); break;
+                case 6: ring_group<6, R>(trm, nt, tid, tile32, xv, acc); break;
+                default: ring_group<7, R>(trm, nt, tid, tile32, xv, acc); break;
+                }
+                trm += nt;
+                // FP32: fold the running group sum into the compensated row
+                // sum every kCompensateGroups groups
+                if (((g + 1) % kCompensateGroups) == 0u) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) acc[j].compensate();
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j].compensate();
+        __syncwarp();
+        if ((tid & 31u) == 0u) mbar_arrive(&empty[stage]);
+        if (++stage == K) {
+            stage = 0;
+            phase ^= 1u;
+        }
+    }
+    C *yt = y + (tile << kTileBitsC128);
+    if (PASSES && accumulate) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            C &out = yt[tid + (j << kLogThreads)];
+            const C v = acc[j].value();
+            out.x += v.x;
+            out.y += v.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) yt[tid + (j << kLogThreads)] = acc[j].value();
+    }
+}
+
 // One thread per row; gathers straight from global memory.
 template <typename R>
 __global__ void k_rowwise(DevSchedule s, const typename Cx<R>::T *__restrict__ x,
@@ -325,8 +552,9 @@ int check_plan(const tcp_mvp_plan *plan) {
 }
 
 int length_error(uint64_t expected, uint64_t actual) {
-    return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH,
-                "expected structure length " + std::to_string(expected) + ", got " + std::to_string(actual));
+    return fail_fields(TCP_ERR_INVALID_STRUCTURE_LENGTH,
+                       "expected structure length " + std::to_string(expected) + ", got " + std::to_string(actual),
+                       expected, actual);
 }
 
 bool overlaps(const void *a, const void *b, size_t bytes) {
@@ -355,22 +583,23 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Step ranges of the source-chunk passes (see DevSchedule::pass_begin): the
 // top kPassBits bits v of each step's outer pattern d, which is
 // non-decreasing in step order because steps are sorted by d.
-void set_passes(DevSchedule &dev, const tcp::Schedule &h, uint32_t nqubits) {
-    const uint32_t nsteps = static_cast<uint32_t>(h.step_info.size() / 4);
-    dev.pass_shift = kNoPasses;
-    for (uint32_t v = 0; v <= kPassChunks; ++v) dev.pass_begin[v] = v == 0 ? 0u : nsteps;
-    if (nqubits < h.tile_bits + kPassBits) return;
-    const uint32_t shift = nqubits - h.tile_bits - kPassBits;
+void set_passes(const std::vector<uint32_t> &step_info, uint32_t tile_bits, uint32_t nqubits, uint32_t *pass_begin,
+                uint32_t *pass_shift) {
+    const uint32_t nsteps = static_cast<uint32_t>(step_info.size() / 4);
+    *pass_shift = kNoPasses;
+    for (uint32_t v = 0; v <= kPassChunks; ++v) pass_begin[v] = v == 0 ? 0u : nsteps;
+    if (tile_bits == 0 || nqubits < tile_bits + kPassBits) return;
+    const uint32_t shift = nqubits - tile_bits - kPassBits;
     uint32_t prev = 0;
     for (uint32_t st = 0; st < nsteps; ++st) {
-        const uint64_t d = static_cast<uint64_t>(h.step_info[4 * st]) | (static_cast<uint64_t>(h.step_info[4 * st + 1]) << 32);
+        const uint64_t d = static_cast<uint64_t>(step_info[4 * st]) | (static_cast<uint64_t>(step_info[4 * st + 1]) << 32);
         const uint32_t v = static_cast<uint32_t>(d >> shift);
         if (v >= kPassChunks || v < prev) return;  // not a sorted schedule: no passes
-        for (uint32_t w = prev + 1; w <= v; ++w) dev.pass_begin[w] = st;
+        for (uint32_t w = prev + 1; w <= v; ++w) pass_begin[w] = st;
         prev = v;
     }
-    for (uint32_t w = prev + 1; w <= kPassChunks; ++w) dev.pass_begin[w] = nsteps;
-    dev.pass_shift = shift;
+    for (uint32_t w = prev + 1; w <= kPassChunks; ++w) pass_begin[w] = nsteps;
+    *pass_shift = shift;
 }
 
 // Lay both schedules out in one device allocation.
@@ -395,7 +624,13 @@ int upload(tcp_mvp_plan *p) {
         add(h.t_wf.data(), h.t_wf.size() * 4, reinterpret_cast<const void **>(&ds->dev.t_wf));
         ds->dev.nsteps = static_cast<uint32_t>(h.step_info.size() / 4);
         ds->dev.tile_bits = h.tile_bits;
-        set_passes(ds->dev, h, p->nqubits);
+        set_passes(h.step_info, h.tile_bits, p->nqubits, ds->dev.pass_begin, &ds->dev.pass_shift);
+        tcp::RingSchedule &r = ds->ring;
+        add(r.step_info.data(), r.step_info.size() * 4, reinterpret_cast<const void **>(&ds->dev.ring_info));
+        add(r.blocks_c128.data(), r.blocks_c128.size(), reinterpret_cast<const void **>(&ds->dev.ring128));
+        add(r.blocks_c64.data(), r.blocks_c64.size(), reinterpret_cast<const void **>(&ds->dev.ring64));
+        ds->dev.ring_steps = static_cast<uint32_t>(r.step_info.size() / 4);
+        set_passes(r.step_info, r.tile_bits, p->nqubits, ds->dev.ring_pass_begin, &ds->dev.ring_pass_shift);
         ds->dev.ngroups = static_cast<uint32_t>(h.g_mask.size());
     }
     size_t total = 256;  // error word first
@@ -442,19 +677,58 @@ template <int LOGE, typename R> int set_smem_attr() {
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "cudaFuncSetAttribute");
 }
 
-// Launch one right-hand side.
-// Number of output tiles of the tiled kernel (0 when the plan uses the row
+template <typename R> int set_ring_smem_attr() {
+    constexpr size_t bytes = ring_smem_bytes<R>();
+    cudaError_t e = cudaFuncSetAttribute(k_ring<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ring<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "cudaFuncSetAttribute");
+}
+
+// The ring kernel serves every plan with a ring schedule whose input the TMA
+// engine can address (16-byte aligned).
+bool ring_ok(const tcp_mvp_plan *p, const void *x) {
+    return p->sched.ring.tile_bits == kTileBitsC128 && p->nqubits >= kTileBitsC128 &&
+           (reinterpret_cast<uintptr_t>(x) % 16) == 0;
+}
+
+// Number of output tiles of the tiled kernels (0 when the plan uses the row
 // kernel for these buffers).
 template <typename R>
 uint64_t tiled_tiles(const tcp_mvp_plan *p, const void *x) {
     constexpr int LOGE = sizeof(R) == 8 ? kLogRowsC128 : kLogRowsC64;
     const uint32_t S = kLogThreads + LOGE;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
+    if (ring_ok(p, x)) return p->dim >> kTileBitsC128;
     return (p->nqubits >= S && p->sched.host.tile_bits == S && aligned) ? (p->dim >> S) : 0;
 }
 
-// Apply on `stream`; the tiled kernel writes output tiles [tile0, tile0 +
-// ntiles) (ntiles = 0: all of them).
+// Whether the host path can split the state into kPassChunks parts for the
+// kernel that serves these buffers.
+bool has_passes(const tcp_mvp_plan *p, const void *x) {
+    return (ring_ok(p, x) ? p->sched.dev.ring_pass_shift : p->sched.dev.pass_shift) != kNoPasses;
+}
+
+// Per-device, once: the shared-memory opt-in of the tiled kernels.
+template <typename R> int ensure_smem_attrs(int device) {
+    static std::mutex attr_mutex;
+    static bool attr_done[64] = {};
+    std::lock_guard<std::mutex> lock(attr_mutex);
+    if (device < 0 || device >= 64) return fail(TCP_ERR_WRONG_DEVICE, "device ordinal out of range");
+    if (!attr_done[device]) {
+        constexpr int LOGE = sizeof(R) == 8 ? kLogRowsC128 : kLogRowsC64;
+        int st = set_smem_attr<LOGE, R>();
+        if (st == TCP_OK) st = set_ring_smem_attr<R>();
+        if (st != TCP_OK) return st;
+        attr_done[device] = true;
+    }
+    return TCP_OK;
+}
+
+// Apply on `stream`; the tiled kernels write output tiles [tile0, tile0 +
+// ntiles) (ntiles = 0: all of them).  pass >= 0 runs one source-part pass of
+// the host path, adding to y when `accumulate`.
 template <typename R>
 int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t stream, uint64_t tile0 = 0,
                uint64_t ntiles = 0, int pass = -1, bool accumulate = false) {
@@ -464,18 +738,22 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
     const tcp::DeviceSchedule &ds = p->sched;
     const uint32_t S = kLogThreads + LOGE;
     const bool aligned = (reinterpret_cast<uintptr_t>(x) % 16) == 0;
-    if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
-        // The shared-memory opt-in is a per-device function attribute.
-        static std::mutex attr_mutex;
-        static bool attr_done[64] = {};
-        {
-            std::lock_guard<std::mutex> lock(attr_mutex);
-            if (p->device < 64 && !attr_done[p->device]) {
-                int attr_status = set_smem_attr<LOGE, R>();
-                if (attr_status != TCP_OK) return attr_status;
-                attr_done[p->device] = true;
-            }
+    if (ring_ok(p, x)) {
+        int st = ensure_smem_attrs<R>(p->device);
+        if (st != TCP_OK) return st;
+        const uint64_t tiles = ntiles ? ntiles : (p->dim >> kTileBitsC128) - tile0;
+        const size_t smem = ring_smem_bytes<R>();
+        if (pass >= 0) {
+            k_ring<R, true><<<static_cast<unsigned>(tiles), kRingThreads, smem, stream>>>(
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, static_cast<uint32_t>(pass),
+                accumulate ? 1u : 0u);
+        } else {
+            k_ring<R, false><<<static_cast<unsigned>(tiles), kRingThreads, smem, stream>>>(
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, 0u);
         }
+    } else if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
+        int st = ensure_smem_attrs<R>(p->device);
+        if (st != TCP_OK) return st;
         const uint64_t tiles = ntiles ? ntiles : (p->dim >> S) - tile0;
         const size_t smem = tiled_smem_bytes<LOGE, R>();
         if (pass >= 0) {
@@ -557,7 +835,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     // them.  Smaller applies copy, launch once and copy back on one stream.
     const uint64_t tiles = tiled_tiles<R>(plan, ws.x);
     const uint64_t chunks = tiles >= kHostChunkTiles ? kHostChunks : 1;
-    const bool passes = chunks > 1 && plan->sched.dev.pass_shift != kNoPasses;
+    const bool passes = chunks > 1 && has_passes(plan, ws.x);
     constexpr int kParts = static_cast<int>(kPassChunks);
     cudaStream_t copy_stream = nullptr, in_stream = nullptr;
     cudaEvent_t done[kHostChunks] = {};
@@ -677,20 +955,25 @@ extern "C" int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32
         unsigned __int128 term_bytes = static_cast<unsigned __int128>(term_count) * 32u;
         if (diag >> 64) return fail(TCP_ERR_OVERFLOW, "integer overflow while estimating reusable MVP plan memory");
         if (term_bytes > max_bytes) {
-            return fail(TCP_ERR_MEMORY_LIMIT, "requested " + std::to_string(static_cast<uint64_t>(term_bytes)) +
-                                                  " bytes exceeds memory limit " + std::to_string(max_bytes));
+            return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                                    "requested " + std::to_string(static_cast<uint64_t>(term_bytes)) +
+                                        " bytes exceeds memory limit " + std::to_string(max_bytes),
+                                    tcp::clamp_u64(term_bytes), max_bytes);
         }
         unsigned __int128 construction = diag + 2 * term_bytes + static_cast<unsigned __int128>(p->group_count) * 32u;
         if (construction > max_bytes) {
             std::string req = construction >> 64 ? std::string("more than 2^64")
                                                   : std::to_string(static_cast<uint64_t>(construction));
-            return fail(TCP_ERR_MEMORY_LIMIT, "requested " + req + " bytes exceeds memory limit " + std::to_string(max_bytes));
+            return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                                    "requested " + req + " bytes exceeds memory limit " + std::to_string(max_bytes),
+                                    tcp::clamp_u64(construction), max_bytes);
         }
     }
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (g_num_sms == 0) cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, p->device);
     p->sched.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
+    p->sched.ring = tcp::build_ring_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
     st = upload(p.get());
     if (st) return st;
     if (storage == TCP_STORAGE_EAGER) {
@@ -892,7 +1175,7 @@ int noalloc_scratch(int device, unsigned char **out) {
         g_noalloc_ptr[device] = static_cast<unsigned char *>(p);
     }
     if (!g_noalloc_attr[device]) {
-        int st = set_smem_attr<kLogRowsC128, double>();
+        int st = ensure_smem_attrs<double>(device);
         if (st) return st;
         g_noalloc_attr[device] = true;
     }
@@ -910,10 +1193,12 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     if (result_len != plan->dim) return length_error(plan->dim, result_len);
     if (state == nullptr || result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     if (plan->nqubits > TCP_NOALLOC_MAX_QUBITS) {
-        return fail(TCP_ERR_MEMORY_LIMIT,
-                    "tcp_mvp_apply_into_host_noalloc handles at most " + std::to_string(TCP_NOALLOC_MAX_QUBITS) +
-                        " qubits (static scratch of 2^" + std::to_string(TCP_NOALLOC_MAX_QUBITS) +
-                        " amplitudes per vector); this plan has " + std::to_string(plan->nqubits));
+        return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                                "tcp_mvp_apply_into_host_noalloc handles at most " +
+                                    std::to_string(TCP_NOALLOC_MAX_QUBITS) + " qubits (static scratch of 2^" +
+                                    std::to_string(TCP_NOALLOC_MAX_QUBITS) + " amplitudes per vector); this plan has " +
+                                    std::to_string(plan->nqubits),
+                                plan->dim * 2 * sizeof(double2), 2 * kNoallocMaxDim * sizeof(double2));
     }
     const size_t bytes = plan->dim * sizeof(double2);
     if (overlaps(state, result, bytes)) return fail(TCP_ERR_INVALID_ARGUMENT, "input and output must not overlap");
@@ -931,7 +1216,10 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     if (e != cudaSuccess) return cuda_fail(e, "H2D copy into the static scratch");
     const tcp::DeviceSchedule &ds = plan->sched;
     const uint32_t S = kTileBitsC128;
-    if (plan->nqubits >= S && ds.host.tile_bits == S) {
+    if (ring_ok(plan, dx)) {
+        k_ring<double, false><<<static_cast<unsigned>(plan->dim >> S), kRingThreads, ring_smem_bytes<double>(), s>>>(
+            ds.dev, dx, dy, d_status, 0, 0u, 0u);
+    } else if (plan->nqubits >= S && ds.host.tile_bits == S) {
         const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();
         k_tiled<kLogRowsC128, double, false><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(
             ds.dev, dx, dy, d_status, 0, 0u, 0u);
@@ -949,6 +1237,11 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     if (e != cudaSuccess) return cuda_fail(e, "reading the static scratch status");
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
-    if (h_status & kErrTimeout) return fail(TCP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+    if (h_status & kErrTimeout) {
+        // the kernel gave up before writing every output tile: no stale rows
+        // of an earlier call reach the caller
+        std::memset(result, 0, bytes);
+        return fail(TCP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+    }
     return TCP_OK;
 }

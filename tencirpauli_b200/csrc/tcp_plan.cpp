@@ -14,15 +14,24 @@ namespace tcp {
 
 namespace {
 thread_local std::string g_last_error;
+thread_local int g_last_status = 0;
+thread_local uint64_t g_last_fields[2] = {0, 0};
 std::atomic<long long> g_alloc_count{0};
 }  // namespace
 
 void set_error(const std::string &message) { g_last_error = message; }
 
-int fail(int status, const std::string &message) {
+int fail(int status, const std::string &message) { return fail_fields(status, message, 0, 0); }
+
+int fail_fields(int status, const std::string &message, uint64_t a, uint64_t b) {
     g_last_error = message;
+    g_last_status = status;
+    g_last_fields[0] = a;
+    g_last_fields[1] = b;
     return status;
 }
+
+uint64_t clamp_u64(unsigned __int128 v) { return (v >> 64) ? ~0ull : static_cast<uint64_t>(v); }
 
 bool injected_alloc_failure() {
     const char *env = std::getenv("TCP_FAIL_ALLOC_AFTER");
@@ -39,8 +48,9 @@ int compile_terms(uint32_t nqubits, uint64_t count, uint32_t word_count, const u
     // pauli_action.rs:38-55 -- word-length and dimension checks
     uint32_t expected = packed_word_count(nqubits);
     if (word_count != expected) {
-        return fail(TCP_ERR_INVALID_WORD_LENGTH, "expected " + std::to_string(expected) +
-                                                     " packed words, got " + std::to_string(word_count));
+        return fail_fields(TCP_ERR_INVALID_WORD_LENGTH,
+                           "expected " + std::to_string(expected) + " packed words, got " + std::to_string(word_count),
+                           expected, word_count);
     }
     if (nqubits >= 64) return fail(TCP_ERR_OVERFLOW, "integer overflow while computing dense statevector dimension");
     out.clear();
@@ -50,7 +60,8 @@ int compile_terms(uint32_t nqubits, uint64_t count, uint32_t word_count, const u
     for (uint64_t t = 0; t < count; ++t) {
         double re = coefficients[2 * t], im = coefficients[2 * t + 1];
         if (!std::isfinite(re) || !std::isfinite(im)) {
-            return fail(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite");
+            return fail_fields(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite",
+                               t, 0);
         }
         uint64_t xm = 0, zm = 0;
         uint32_t ny = 0;
@@ -237,6 +248,150 @@ Schedule build_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, 
     return s;
 }
 
+RingSchedule build_ring_schedule(const std::vector<MatrixTerm> &terms, uint32_t nqubits, uint32_t tile_bits,
+                                 uint32_t log_threads) {
+    RingSchedule r;
+    // The ring kernel covers 512 threads x 8 rows per tile, and outer z bits
+    // that fit 32 bits.
+    if (log_threads != 9 || tile_bits != 12 || nqubits < tile_bits || nqubits - tile_bits > 32) return r;
+    const uint32_t S = tile_bits, L = log_threads;
+    const uint64_t inner = (1ull << S) - 1, tmask = (1ull << L) - 1;
+    r.tile_bits = S;
+    r.log_threads = L;
+
+    // One record per real or imaginary weight part; canonical order inside a
+    // group, real part before imaginary part.
+    struct Item {
+        uint64_t d;
+        uint32_t m_lo, jh;
+        uint64_t mask;
+        uint64_t z;
+        uint64_t canon;
+        uint32_t imag;
+        double w;
+    };
+    std::vector<Item> items;
+    items.reserve(terms.size() + 8);
+    for (uint64_t i = 0; i < terms.size(); ++i) {
+        const MatrixTerm &t = terms[i];
+        const uint64_t d = t.x_mask >> S;
+        const uint32_t m_lo = static_cast<uint32_t>(t.x_mask & tmask);
+        const uint32_t jh = static_cast<uint32_t>((t.x_mask & inner) >> L);
+        if (t.w_re != 0.0 || t.w_im == 0.0) items.push_back({d, m_lo, jh, t.x_mask, t.z_mask, i, 0u, t.w_re});
+        if (t.w_im != 0.0) items.push_back({d, m_lo, jh, t.x_mask, t.z_mask, i, 1u, t.w_im});
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
+        if (a.d != b.d) return a.d < b.d;
+        if (a.m_lo != b.m_lo) return a.m_lo < b.m_lo;
+        if (a.jh != b.jh) return a.jh < b.jh;
+        return a.canon < b.canon;
+    });
+
+    struct PGroup {
+        uint32_t a = 0;
+        std::vector<size_t> items;
+    };
+    struct PCoset {
+        uint32_t m_lo = 0, jh = 0;
+        std::vector<PGroup> groups;
+    };
+    std::vector<PCoset> pend;
+    size_t pend_groups = 0, pend_terms = 0;
+    uint64_t cur_d = 0;
+    auto block_bytes = [](size_t c, size_t g, size_t t) { return 16 + 16 * c + (4 * g + 15) / 16 * 16 + 16 * t; };
+    auto flush = [&]() {
+        if (pend.empty()) return;
+        const size_t off = r.blocks_c128.size();
+        const size_t terms_off = 16 + 16 * pend.size() + (4 * pend_groups + 15) / 16 * 16;
+        put(r.blocks_c128, static_cast<uint32_t>(pend.size()));
+        put(r.blocks_c128, static_cast<uint32_t>(pend_groups));
+        put(r.blocks_c128, static_cast<uint32_t>(terms_off / 16));
+        put(r.blocks_c128, uint32_t(0));
+        for (auto &c : pend) {
+            put(r.blocks_c128, c.m_lo);
+            put(r.blocks_c128, c.jh);
+            put(r.blocks_c128, static_cast<uint32_t>(c.groups.size()));
+            put(r.blocks_c128, uint32_t(0));
+        }
+        for (auto &c : pend)
+            for (auto &g : c.groups) put(r.blocks_c128, g.a | static_cast<uint32_t>(g.items.size() << 4));
+        while ((r.blocks_c128.size() - off) % 16) r.blocks_c128.push_back(0);
+        for (auto &c : pend) {
+            for (auto &g : c.groups) {
+                for (size_t k : g.items) {
+                    const Item &it = items[k];
+                    const uint64_t zt = it.z >> S;
+                    const uint32_t zlo = static_cast<uint32_t>(it.z & tmask);
+                    const uint32_t zj = static_cast<uint32_t>((it.z & inner) >> L);
+                    uint32_t pattern = 0;
+                    for (uint32_t j = 0; j < 8; ++j) pattern |= (static_cast<uint32_t>(__builtin_popcount(zj & j)) & 1u) << j;
+                    const bool flip = ((__builtin_popcountll(zt & cur_d) + __builtin_popcount(zlo & it.m_lo) +
+                                        __builtin_popcount(zj & it.jh)) & 1) != 0;
+                    const double w = flip ? -it.w : it.w;
+                    put(r.blocks_c128, zlo | (pattern << 9) | (it.imag << 17));
+                    put(r.blocks_c128, static_cast<uint32_t>(zt));
+                    put(r.blocks_c128, w);
+                }
+            }
+        }
+        const size_t bytes = r.blocks_c128.size() - off;
+        r.max_block_bytes = std::max<uint32_t>(r.max_block_bytes, static_cast<uint32_t>(bytes));
+        r.step_info.push_back(static_cast<uint32_t>(cur_d));
+        r.step_info.push_back(static_cast<uint32_t>(cur_d >> 32));
+        r.step_info.push_back(static_cast<uint32_t>(off / 16));
+        r.step_info.push_back(static_cast<uint32_t>(bytes / 16));
+        r.cosets += pend.size();
+        pend.clear();
+        pend_groups = pend_terms = 0;
+    };
+    bool have = false;
+    for (size_t k = 0; k < items.size(); ++k) {
+        const Item &it = items[k];
+        if (!have || it.d != cur_d) {
+            flush();
+            cur_d = it.d;
+            have = true;
+        }
+        bool new_coset = pend.empty() || pend.back().m_lo != it.m_lo;
+        bool new_group = new_coset || items[pend.back().groups.back().items.back()].mask != it.mask;
+        if (block_bytes(pend.size() + new_coset, pend_groups + new_group, pend_terms + 1) > kRingBlockBytes) {
+            flush();
+            new_coset = new_group = true;
+        }
+        if (new_coset) {
+            PCoset c;
+            c.m_lo = it.m_lo;
+            c.jh = it.jh;
+            pend.push_back(c);
+        }
+        if (new_group) {
+            PGroup g;
+            g.a = it.jh ^ pend.back().jh;
+            pend.back().groups.push_back(g);
+            ++pend_groups;
+        }
+        pend.back().groups.back().items.push_back(k);
+        ++pend_terms;
+    }
+    flush();
+    // complex64 blocks: the same layout with the weight rounded to FP32
+    r.blocks_c64 = r.blocks_c128;
+    for (size_t i = 0; i + 4 <= r.step_info.size(); i += 4) {
+        const size_t off = static_cast<size_t>(r.step_info[i + 2]) * 16;
+        const size_t bytes = static_cast<size_t>(r.step_info[i + 3]) * 16;
+        uint32_t terms_off;
+        std::memcpy(&terms_off, &r.blocks_c128[off + 8], 4);
+        for (size_t p = off + static_cast<size_t>(terms_off) * 16; p < off + bytes; p += 16) {
+            double w;
+            std::memcpy(&w, &r.blocks_c128[p + 8], 8);
+            const float f = static_cast<float>(w);
+            std::memcpy(&r.blocks_c64[p + 8], &f, 4);
+            std::memset(&r.blocks_c64[p + 12], 0, 4);
+        }
+    }
+    return r;
+}
+
 }  // namespace tcp
 
 // ---------------------------------------------------------------------------
@@ -268,14 +423,17 @@ extern "C" int tcp_pauli_canonicalize(uint32_t nqubits, uint64_t count, const ui
     for (uint64_t t = 0; t < count; ++t) {
         if (!std::isfinite(coefficients[2 * t]) || !std::isfinite(coefficients[2 * t + 1])) {
             if (bad_index) *bad_index = t;
-            return fail(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite");
+            return fail_fields(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite",
+                               t, 0);
         }
         for (uint32_t q = 0; q < nqubits; ++q) {
             uint8_t c = codes[t * nqubits + q];
             if (c > 3) {
                 if (bad_index) *bad_index = q;
-                return fail(TCP_ERR_INVALID_CODE,
-                            "invalid Pauli code " + std::to_string(c) + " at index " + std::to_string(q) + "; expected 0..=3");
+                return fail_fields(TCP_ERR_INVALID_CODE,
+                                   "invalid Pauli code " + std::to_string(c) + " at index " + std::to_string(q) +
+                                       "; expected 0..=3",
+                                   c, q);
             }
         }
     }
@@ -363,3 +521,11 @@ extern "C" size_t tcp_last_error(char *buffer, size_t capacity) {
 }
 
 extern "C" int tcp_abi_version(void) { return TCP_ABI_VERSION; }
+
+extern "C" int tcp_last_error_fields(uint64_t *fields) {
+    if (fields != nullptr) {
+        fields[0] = tcp::g_last_fields[0];
+        fields[1] = tcp::g_last_fields[1];
+    }
+    return tcp::g_last_status;
+}

@@ -13,6 +13,7 @@ namespace tcp {
 
 struct DeviceSchedule {
     Schedule host;
+    RingSchedule ring;  // k_ring's schedule (tile_bits = 0: the plan does not use it)
     tcpdev::DevSchedule dev{};
 };
 

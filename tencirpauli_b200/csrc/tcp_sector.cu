@@ -92,8 +92,9 @@ std::string leak_message(uint64_t source, uint32_t expected, uint32_t actual) {
 int rank_packed(uint32_t n, uint32_t k, const uint64_t *words, uint32_t wc, uint64_t &rank) {
     uint32_t expected = word_count_of(n);
     if (wc != expected) {
-        return fail(TCP_ERR_INVALID_WORD_LENGTH,
-                    "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc));
+        return tcp::fail_fields(TCP_ERR_INVALID_WORD_LENGTH,
+                                "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc),
+                                expected, wc);
     }
     if (n % 64 && wc && (words[wc - 1] >> (n % 64))) {
         return fail(TCP_ERR_INVALID_INDEX, "invalid sector index: packed basis word has nonzero padding bits");
@@ -118,8 +119,9 @@ int unrank_packed(uint32_t n, uint32_t k, uint64_t dim, uint64_t index, uint64_t
     if (index >= dim) return fail(TCP_ERR_INVALID_INDEX, "invalid sector index: restricted basis index is out of range");
     uint32_t expected = word_count_of(n);
     if (wc != expected) {
-        return fail(TCP_ERR_INVALID_WORD_LENGTH,
-                    "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc));
+        return tcp::fail_fields(TCP_ERR_INVALID_WORD_LENGTH,
+                                "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc),
+                                expected, wc);
     }
     std::fill(words, words + wc, 0ull);
     uint64_t r = index;
@@ -156,8 +158,9 @@ int compile_u1(uint32_t n, uint64_t count, uint32_t wc, const uint64_t *xw, cons
                uint32_t W, U1Terms &out) {
     uint32_t expected = word_count_of(n);
     if (wc != expected) {
-        return fail(TCP_ERR_INVALID_WORD_LENGTH,
-                    "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc));
+        return tcp::fail_fields(TCP_ERR_INVALID_WORD_LENGTH,
+                                "expected " + std::to_string(expected) + " packed words, got " + std::to_string(wc),
+                                expected, wc);
     }
     std::map<std::vector<uint64_t>, uint32_t> lookup;
     std::vector<uint32_t> group_of(count);
@@ -168,7 +171,8 @@ int compile_u1(uint32_t n, uint64_t count, uint32_t wc, const uint64_t *xw, cons
     for (uint64_t t = 0; t < count; ++t) {
         double re = coef[2 * t], im = coef[2 * t + 1];
         if (!std::isfinite(re) || !std::isfinite(im)) {
-            return fail(TCP_ERR_NON_FINITE_COEFFICIENT, "coefficient at index " + std::to_string(t) + " is not finite");
+            return tcp::fail_fields(TCP_ERR_NON_FINITE_COEFFICIENT,
+                                    "coefficient at index " + std::to_string(t) + " is not finite", t, 0);
         }
         uint32_t ny = 0;
         for (uint32_t q = 0; q < n; ++q) {
@@ -1062,7 +1066,7 @@ int scan_leakage(const tcp_u1_plan *p) {
         if ((words[q / 64] >> (q % 64)) & 1) b[(p->n - 1 - q) / 64] |= 1ull << ((p->n - 1 - q) % 64);
     uint32_t actual = 0;
     for (uint32_t i = 0; i < p->W; ++i) actual += static_cast<uint32_t>(__builtin_popcountll(b[i] ^ p->terms.gx[g * p->W + i]));
-    return fail(TCP_ERR_SECTOR_LEAKAGE, leak_message(source, p->k, actual));
+    return tcp::fail_fields(TCP_ERR_SECTOR_LEAKAGE, leak_message(source, p->k, actual), source, actual);
 }
 
 // One device allocation: choose table, rank tables, groups, terms, basis.
@@ -1464,8 +1468,8 @@ template <typename R>
 int apply_host(const tcp_u1_plan *plan, const R *state, uint64_t state_len, R *result, uint64_t result_len) {
     int st = check_u1(plan);
     if (st) return st;
-    if (state_len != plan->dim) return tcp::fail(TCP_ERR_INVALID_STRUCTURE_LENGTH, "expected structure length " + std::to_string(plan->dim) + ", got " + std::to_string(state_len));
-    if (result_len != plan->dim) return tcp::fail(TCP_ERR_INVALID_STRUCTURE_LENGTH, "expected structure length " + std::to_string(plan->dim) + ", got " + std::to_string(result_len));
+    if (state_len != plan->dim) return tcp::length_error(plan->dim, state_len);
+    if (result_len != plan->dim) return tcp::length_error(plan->dim, result_len);
     if (state == nullptr || result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     const size_t bytes = plan->dim * 2 * sizeof(R);
     auto pa = reinterpret_cast<uintptr_t>(state), pb = reinterpret_cast<uintptr_t>(result);
@@ -1590,7 +1594,10 @@ extern "C" int tcp_u1_basis_words(uint32_t nqubits, uint32_t particle_number, ui
     const uint32_t wc = nqubits <= 64 ? 1 : word_count_of(nqubits);
     const unsigned __int128 count = static_cast<unsigned __int128>(dim) * wc;
     const unsigned __int128 bytes = count * 8;
-    if (bytes > max_bytes) return fail(TCP_ERR_MEMORY_LIMIT, "requested " + bytes_str(bytes) + " bytes exceeds memory limit " + std::to_string(max_bytes));
+    if (bytes > max_bytes)
+        return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                                "requested " + bytes_str(bytes) + " bytes exceeds memory limit " + std::to_string(max_bytes),
+                                tcp::clamp_u64(bytes), max_bytes);
     if (count > capacity) return fail(TCP_ERR_INVALID_ARGUMENT, "basis output buffer is too small");
     if (dim && out == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null output");
     const uint32_t pw = word_count_of(nqubits);
@@ -1622,7 +1629,9 @@ extern "C" int tcp_pauli_number_commutator(uint32_t nqubits, uint64_t term_count
     if (out_nonzero == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null output");
     const uint32_t wc = word_count_of(nqubits);
     if (word_count != wc) {
-        return fail(TCP_ERR_INVALID_WORD_LENGTH, "expected " + std::to_string(wc) + " packed words, got " + std::to_string(word_count));
+        return tcp::fail_fields(TCP_ERR_INVALID_WORD_LENGTH,
+                                "expected " + std::to_string(wc) + " packed words, got " + std::to_string(word_count), wc,
+                                word_count);
     }
     if (term_count && (x_words == nullptr || z_words == nullptr || coefficients == nullptr)) {
         return fail(TCP_ERR_INVALID_ARGUMENT, "null term arrays");
@@ -1706,14 +1715,20 @@ extern "C" int tcp_u1_plan_create(uint32_t nqubits, uint32_t particle_number, ui
     if (storage == TCP_STORAGE_LAZY) {
         p->estimated = estimate_compiled(p.get());
         if (p->estimated > max_bytes) {
-            return fail(TCP_ERR_MEMORY_LIMIT, "requested " + std::to_string(p->estimated) + " bytes exceeds memory limit " + std::to_string(max_bytes));
+            return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                                    "requested " + std::to_string(p->estimated) + " bytes exceeds memory limit " +
+                                        std::to_string(max_bytes),
+                                    p->estimated, max_bytes);
         }
     } else {
         unsigned __int128 bytes = 0;
         st = estimate_eager(p.get(), bytes);
         if (st) return st;
         if (bytes > max_bytes) {
-            return fail(TCP_ERR_MEMORY_LIMIT, "requested " + bytes_str(bytes) + " bytes exceeds memory limit " + std::to_string(max_bytes));
+            return tcp::fail_fields(TCP_ERR_MEMORY_LIMIT,
+                                    "requested " + bytes_str(bytes) + " bytes exceeds memory limit " +
+                                        std::to_string(max_bytes),
+                                    tcp::clamp_u64(bytes), max_bytes);
         }
         p->estimated = estimate_compiled(p.get());
     }
@@ -1782,7 +1797,7 @@ extern "C" int tcp_u1_apply_into_device(const tcp_u1_plan *plan, const void *d_s
                                         uint32_t nrhs, int dtype, void *stream) {
     int st = check_u1(plan);
     if (st) return st;
-    if (len != plan->dim) return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH, "expected structure length " + std::to_string(plan->dim) + ", got " + std::to_string(len));
+    if (len != plan->dim) return tcp::length_error(plan->dim, len);
     if (dtype != TCP_DTYPE_C128 && dtype != TCP_DTYPE_C64) return fail(TCP_ERR_INVALID_ARGUMENT, "unknown dtype");
     if (nrhs == 0) return TCP_OK;
     if (d_state == nullptr || d_result == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
@@ -1803,7 +1818,7 @@ extern "C" int tcp_u1_apply_into_device(const tcp_u1_plan *plan, const void *d_s
 extern "C" int tcp_u1_diagonal_device(const tcp_u1_plan *plan, void *d_diag, uint64_t len, void *stream) {
     int st = check_u1(plan);
     if (st) return st;
-    if (len != plan->dim) return fail(TCP_ERR_INVALID_STRUCTURE_LENGTH, "expected structure length " + std::to_string(plan->dim) + ", got " + std::to_string(len));
+    if (len != plan->dim) return tcp::length_error(plan->dim, len);
     if (d_diag == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (plan->W > 1) {

@@ -56,13 +56,21 @@ def _to_codes(n: int, x: np.ndarray, z: np.ndarray) -> np.ndarray:
     return codes
 
 
-def jordan_wigner_integrals(h: np.ndarray, g: np.ndarray, tol: float = 0.0) -> Tuple[np.ndarray, np.ndarray]:
+def jordan_wigner_integrals(
+    h: np.ndarray, g: np.ndarray, tol: float = 0.0, constant: complex = 0.0
+) -> Tuple[np.ndarray, np.ndarray]:
     """Pauli code rows and coefficients (not yet canonical) of
-    sum h_pq a†_p a_q + 1/2 sum g_pqrs a†_p a†_q a_s a_r."""
+    constant + sum h_pq a†_p a_q + 1/2 sum g_pqrs a†_p a†_q a_s a_r (the
+    constant is the identity word, as the reference keeps the nuclear
+    constant of ``FermionOperator.from_integrals``)."""
     n = h.shape[0]
     if n > 64:
         raise ValueError("at most 64 modes")
     words_x, words_z, coeffs = [], [], []
+    if constant != 0:
+        words_x.append(np.zeros(1, dtype=np.uint64))
+        words_z.append(np.zeros(1, dtype=np.uint64))
+        coeffs.append(np.asarray([constant], dtype=np.complex128))
     # one-body
     p, q = np.nonzero(np.abs(h) > tol)
     if p.size:

@@ -16,12 +16,15 @@ random streams of the reference tests that pin the MVP path:
 * ``tests/test_native_abi.py:84-120``         H = 2Z + I, apply([1,2]) == [3,-2]
 * ``tests/test_pauli_operator.py:23-30,223-238`` canonical order / aggregation
 * ``crates/tencir-pauli-core/src/tests.rs:25-37,121-158`` mvp_test_operator
+* ``tests/test_integral_ingestion.py:11-38``   spin-orbital integrals -> the
+  expected fermionic terms (the 1/2 two-body factor, index order, constant)
 
 Only the fixtures are committed; the tests never read the reference checkout.
 """
 
 from __future__ import annotations
 
+import argparse
 import os
 import sys
 
@@ -147,8 +150,51 @@ def main(reference_root: str) -> None:
         b_expected_codes=np.asarray([[0, 0], [3, 1]], dtype=np.uint8),
         b_expected_coefficients=np.asarray([2.0, 1.0 - 0.25j], dtype=np.complex128),
     )
-    print(f"wrote {len(out) + 1} fixtures to {HERE}")
+    write_integral_known_answer()
+    print(f"wrote {len(out) + 2} fixtures to {HERE}")
+
+
+# Fermionic ladder actions in the term arrays below.
+CREATE, ANNIHILATE = 1, 0
+
+
+def write_integral_known_answer() -> None:
+    """tests/test_integral_ingestion.py:11-38: FermionOperator.from_integrals
+    of these spin-orbital integrals equals the listed fermionic terms (one-body
+    h_pq a+_p a_q, two-body 1/2 g_pqrs a+_p a+_q a_s a_r, constant kept).  The
+    terms are stored as (mode, action) rows padded with -1."""
+    one_body = np.array([[1.0, 0.2], [0.2, -0.4]], dtype=np.float64)
+    two_body = np.zeros((2, 2, 2, 2), dtype=np.float64)
+    two_body[0, 1, 0, 1] = 2.0
+    terms = [
+        ((), 1.25),
+        (((0, CREATE), (0, ANNIHILATE)), 1.0),
+        (((0, CREATE), (1, ANNIHILATE)), 0.2),
+        (((1, CREATE), (0, ANNIHILATE)), 0.2),
+        (((1, CREATE), (1, ANNIHILATE)), -0.4),
+        (((0, CREATE), (1, CREATE), (1, ANNIHILATE), (0, ANNIHILATE)), 1.0),
+    ]
+    ops = np.full((len(terms), 4, 2), -1, dtype=np.int64)
+    for i, (word, _) in enumerate(terms):
+        for j, (mode, action) in enumerate(word):
+            ops[i, j] = (mode, action)
+    np.savez(
+        os.path.join(HERE, "integral_known_answer.npz"),
+        one_body=one_body,
+        two_body=two_body,
+        constant=np.float64(1.25),
+        term_ops=ops,
+        term_coefficients=np.asarray([c for _, c in terms], dtype=np.complex128),
+    )
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("reference_root", help="path of the TenCirPauli reference checkout")
+    parser.add_argument("--only-integrals", action="store_true",
+                        help="write only the integral known answer (its data is literal, no checkout is read)")
+    ns = parser.parse_args()
+    if ns.only_integrals:
+        write_integral_known_answer()
+    else:
+        main(ns.reference_root)

@@ -96,6 +96,33 @@ def test_last_error_is_thread_local_text() -> None:
     assert "invalid Pauli code 9" in _native.last_error()
 
 
+def test_last_error_fields_rebuild_the_pauli_error_variant() -> None:
+    """tcp_last_error_fields returns the numeric fields of the PauliError
+    variant (crates/tencir-pauli-core/src/error.rs:5-74) beside the status."""
+    with pytest.raises(ValueError):
+        _native.canonicalize(2, np.asarray([[1, 4]], np.uint8), np.asarray([1.0 + 0j]))
+    assert _native.last_error_fields() == (_native.TCP_ERR_INVALID_CODE, 4, 1)
+    with pytest.raises(ValueError):
+        _native.canonicalize(1, np.asarray([[1], [2]], np.uint8), np.asarray([1.0 + 0j, np.nan + 0j]))
+    assert _native.last_error_fields() == (_native.TCP_ERR_NON_FINITE_COEFFICIENT, 1, 0)
+    lib = _native.load_library()
+    x = np.asarray([1], dtype=np.uint64)
+    c = np.asarray([1.0, 0.0], dtype=np.float64)
+    p64 = ctypes.POINTER(ctypes.c_uint64)
+    pf = ctypes.POINTER(ctypes.c_double)
+    handle = ctypes.c_void_p(None)
+    assert lib.tcp_mvp_plan_create(2, 1, 3, x.ctypes.data_as(p64), x.ctypes.data_as(p64), c.ctypes.data_as(pf), 0, 0,
+                                   ctypes.byref(handle)) == _native.TCP_ERR_INVALID_WORD_LENGTH
+    assert _native.last_error_fields() == (_native.TCP_ERR_INVALID_WORD_LENGTH, 1, 3)
+    # eager budget: one group on 30 qubits needs 2^30 * 16 + 2 * 32 + 32 bytes
+    assert lib.tcp_mvp_plan_create(30, 1, 1, x.ctypes.data_as(p64), x.ctypes.data_as(p64), c.ctypes.data_as(pf),
+                                   _native.TCP_STORAGE_EAGER, 1000, ctypes.byref(handle)) == _native.TCP_ERR_MEMORY_LIMIT
+    assert _native.last_error_fields() == (_native.TCP_ERR_MEMORY_LIMIT, (1 << 30) * 16 + 96, 1000)
+    assert lib.tcp_mvp_plan_create(64, 1, 1, x.ctypes.data_as(p64), x.ctypes.data_as(p64), c.ctypes.data_as(pf), 0, 0,
+                                   ctypes.byref(handle)) == _native.TCP_ERR_OVERFLOW
+    assert _native.last_error_fields() == (_native.TCP_ERR_OVERFLOW, 0, 0)
+
+
 def test_eager_budget_is_checked_before_any_device_use() -> None:
     # hamiltonian.rs:84-119: G * 2^n * 16 diagonal bytes against max_bytes
     lib = _native.load_library()
@@ -174,3 +201,16 @@ def test_solver_kernel_limits_are_checked_before_any_launch() -> None:
     assert lib.tcp_block_combine(dummy, c64, 192, dummy, 17, 0, 1.0, 0.0, dummy, c64, None) == 0
     assert lib.tcp_block_combine(dummy, c128, 8, dummy, 0, 1024, 1.0, 0.0, dummy, c128, None) == 0
     assert lib.tcp_block_combine(None, c128, 8, dummy, 4, 1024, 1.0, 0.0, dummy, c128, None) == bad
+
+
+def test_noalloc_entry_point_names_no_allocating_routine() -> None:
+    """The allocation-free host apply and its set-up name no allocating
+    routine.  Its GPU test makes the library's own allocator fail; this source
+    check also covers direct CUDA allocation calls added later."""
+    path = os.path.join(ROOT, "tencirpauli_b200", "csrc", "tcp_mvp.cu")
+    src = open(path).read()
+    start = src.index("int noalloc_scratch(int device, unsigned char **out)")
+    body = src[start:]
+    forbidden = ("cudaMalloc", "cudaFree", "dev_malloc", "cudaHostAlloc", "cudaMallocHost", "malloc(", "new ")
+    for name in forbidden:
+        assert name not in body, f"{name} appears in the allocation-free path"

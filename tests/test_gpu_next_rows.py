@@ -36,9 +36,22 @@ def test_backend_plan_host_and_device_paths() -> None:
     y = f(x)
     assert y.device.type == "cuda" and y.dtype == torch.complex128
     np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
-    # a DLPack capsule from another producer takes the same path
-    y2 = plan.apply(torch.utils.dlpack.to_dlpack(x) if False else x)
-    assert torch.equal(y2, y)
+    # DLPack from another producer: an object that only speaks the protocol
+    # (as CuPy or JAX arrays do), and a bare capsule, take the same path
+    class Foreign:
+        def __init__(self, t):
+            self._t = t
+
+        def __dlpack__(self, *args, **kwargs):
+            return self._t.__dlpack__(*args, **kwargs)
+
+        def __dlpack_device__(self):
+            return self._t.__dlpack_device__()
+
+    y2 = plan.apply(Foreign(x))
+    assert isinstance(y2, torch.Tensor) and torch.equal(y2, y)
+    y3 = f(torch.utils.dlpack.to_dlpack(x.clone()))
+    assert torch.equal(y3, y)
     block = torch.stack([x, 2 * x]).to(torch.complex64)
     yb = f(block)
     assert yb.shape == block.shape and yb.dtype == torch.complex64

@@ -6,6 +6,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+from conftest import load_golden
 from oracle import oracle
 from tencirpauli_b200 import PauliOperator
 from tencirpauli_b200.backend import BackendMVPPlan
@@ -54,6 +55,31 @@ def test_jordan_wigner_matches_dense_ladder_construction(n: int, seed: int) -> N
                     H += 0.5 * g[p, q, r, s] * ad[p] @ ad[q] @ a[s] @ a[r]
     np.testing.assert_allclose(_dense_from_op(op), H, rtol=1e-12, atol=1e-13)
     assert np.allclose(H, H.conj().T)  # Hermitian with the 8-fold symmetric integrals
+
+
+def test_integral_known_answer_of_the_reference() -> None:
+    """The reference's integral convention (tests/test_integral_ingestion.py:11-38
+    of the reference): the mapped operator equals the listed fermionic terms --
+    1/2 on the two-body sum, a+_p a+_q a_s a_r index order, constant kept."""
+    k = load_golden("integral_known_answer")
+    h, g, constant = k["one_body"], k["two_body"], complex(k["constant"])
+    codes, coeffs = jordan_wigner_integrals(h, g, constant=constant)
+    op = PauliOperator.from_code_arrays(codes, coeffs)
+    n = h.shape[0]
+    a = [_ladder_dense(n, p) for p in range(n)]
+    expected = np.zeros((1 << n, 1 << n), dtype=np.complex128)
+    for ops, c in zip(k["term_ops"], k["term_coefficients"]):
+        m = np.eye(1 << n, dtype=np.complex128)
+        for mode, action in ops:
+            if mode < 0:
+                break
+            m = m @ (a[mode].conj().T if action == 1 else a[mode])
+        expected += c * m
+    np.testing.assert_allclose(_dense_from_op(op), expected, rtol=0, atol=1e-15)
+    # without the constant the operator moves by exactly -constant * I
+    codes0, coeffs0 = jordan_wigner_integrals(h, g)
+    dense0 = _dense_from_op(PauliOperator.from_code_arrays(codes0, coeffs0))
+    np.testing.assert_allclose(dense0 + constant * np.eye(1 << n), expected, rtol=0, atol=1e-15)
 
 
 def test_integral_symmetries() -> None:
