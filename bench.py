@@ -9,14 +9,16 @@ L2-normalised).  A step is one y = H x over the whole 2^28 state.
 Metric: amplitude-terms/s = T_canonical * 2^n * (vectors per step) / step time.
 ``value`` is device time (CUDA events on the launching stream, inputs resident
 in HBM, 4 GiB vectors > L2 so no flush is needed); ``e2e`` is the same metric
-through the public host ``apply_into`` path (pinned host buffers, H2D + kernel
-+ D2H in every step).  ``--impl reference`` times the reference's CPU
-algorithm (the C restatement of the Rust TermDirect loop, all host cores) on a
-bounded row sample of the same workload.
+through the public host ``apply_into`` path (H2D + kernel + D2H in every
+step).  ``--impl reference`` times the reference's CPU algorithm (the C
+restatement of the Rust TermDirect loop, all host cores) in fixed blocks of
+rows of the same workload.
 
-Multi-GPU (``torchrun --nproc-per-node N``): one independent state per rank
-(weak scaling, no collective on the data path); the step time is the max over
-ranks.
+Multi-GPU (``torchrun --nproc-per-node N``): the one n = 28 state is sharded
+over the ranks by its top index bits (strong scaling; pairwise shard
+exchanges over NCCL, double-buffered against the applies); ``--replicas``
+instead runs one independent state per rank (weak scaling, no collective on
+the data path).  The step time is the max over ranks.
 """
 
 from __future__ import annotations
@@ -731,6 +733,114 @@ def run_solver(args: argparse.Namespace) -> None:
     }), flush=True)
 
 
+def run_sharded(args: argparse.Namespace, world: int, rank: int) -> None:
+    """The state-sharded MVP (tencirpauli_b200/sharded.py) on ``world`` GPUs
+    over NCCL: the same n = ``--nqubits`` workload split by its top log2(world)
+    index bits, one shard per rank (strong scaling: total work fixed).  A step
+    is one y = H x over the whole state: the local apply plus one pairwise
+    shard exchange per top-bit pattern, each partner's contribution added into
+    y by the kernel; exchanges are double-buffered so they overlap the applies.
+    The step time is the max over ranks of the CUDA-event time."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from tencirpauli_b200 import workloads
+    from tencirpauli_b200.sharded import ShardedMVP
+
+    if world & (world - 1):
+        raise SystemExit("the sharded MVP needs a power-of-two number of GPUs")
+    op = build_operator(args)
+    n, T, dim = op.nqubits, op.term_count, 1 << op.nqubits
+    mvp = ShardedMVP(op, timeout_s=120.0)
+    cdtype = torch.complex128 if args.dtype == "c128" else torch.complex64
+    elem = 16 if args.dtype == "c128" else 8
+    x = workloads.random_state_device(mvp.local_qubits, seed=args.seed + rank, dtype=cdtype)
+    y = torch.empty_like(x)
+    bufs = mvp.receive_buffers(x)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        mvp.apply(x, y, bufs)
+    torch.cuda.synchronize()
+    dist.barrier()
+    sampler = ClockSampler(_smi_id(torch.cuda.current_device()))
+    sampler.start()
+    time.sleep(0.3)
+    t_begin, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t_begin.record(stream)
+    for _ in range(args.steps):
+        mvp.apply(x, y, bufs)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    for plan in mvp._plans.values():
+        plan._native_plan.device_status()
+    ms = torch.tensor([t_begin.elapsed_time(t_end) / args.steps], device="cuda", dtype=torch.float64)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_per_step = float(ms.item())
+    value = T * dim / (ms_per_step / 1e3)
+    # end to end: each rank's shard from page-locked host memory, the sharded
+    # apply, the shard of y back to the host; max over ranks
+    xh = torch.empty(mvp.shard_len, dtype=cdtype, pin_memory=True)
+    yh = torch.empty(mvp.shard_len, dtype=cdtype, pin_memory=True)
+    xh.copy_(x)
+    xd = torch.empty_like(x)
+    e2e = []
+    for _ in range(max(1, args.e2e_steps)):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xd.copy_(xh, non_blocking=True)
+        mvp.apply(xd, y, bufs)
+        yh.copy_(y, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    e2e_t = torch.tensor([statistics.median(e2e)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    # size-independent check: <a, H b> == <H a, b> across all shards
+    a = workloads.random_state_device(mvp.local_qubits, seed=args.seed + 1000 + rank, dtype=cdtype)
+    ha = torch.empty_like(a)
+    mvp.apply(a, ha, bufs)
+    mvp.apply(x, y, bufs)
+    dots = torch.stack([torch.vdot(a, y), torch.vdot(ha, x)]).to(torch.complex128)
+    dist.all_reduce(dots)
+    herm = abs(complex(dots[0]) - complex(dots[1])) / max(abs(complex(dots[0])), 1e-300)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f64" if args.dtype == "c128" else "f32",
+        "data": "synthetic",
+        "config": dict(workload_config(args, op), parallelism=f"state sharded over {world} GPUs by the top "
+                       f"{world.bit_length() - 1} index bits", shard_amplitudes=mvp.shard_len,
+                       exchange_patterns=len(mvp.patterns)),
+        "e2e": {"value": T * dim / float(e2e_t.item()), "unit": UNIT, "h2d_bytes_per_step": dim * elem,
+                "d2h_bytes_per_step": dim * elem, "ms_per_step": 1e3 * float(e2e_t.item()),
+                "note": "bytes summed over ranks; each rank copies its own shard"},
+        "gpu_launches": args.steps * (len(mvp.patterns) + 1),
+        "clocks": clocks,
+        "accuracy": {"hermiticity_rel": herm},
+        "manifest": manifest(),
+    }
+    for b in bufs:
+        del b
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--weights", default=None)
@@ -759,6 +869,8 @@ def main() -> None:
     parser.add_argument("--reference-full-pass", type=int, default=1,
                         help="reference arm: also time one full pass over the state (1) or not (0)")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--replicas", action="store_true",
+                        help="with several GPUs: one independent state per GPU instead of one sharded state")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -792,6 +904,9 @@ def main() -> None:
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if not args.replicas:
+            run_sharded(args, world, rank)
+            return
 
     from tencirpauli_b200 import workloads
 
@@ -842,28 +957,38 @@ def main() -> None:
     amp_terms = T * dim
     value = amp_terms * world / (ms_per_step / 1000.0)
 
-    # end to end through the public host apply_into (pinned host buffers)
+    # end to end through the public host apply_into: ordinary NumPy buffers
+    # (what the reference's facade passes) for the headline, page-locked
+    # buffers beside it
     x_host = torch.empty(dim, dtype=cdtype, pin_memory=True)
     y_host = torch.empty(dim, dtype=cdtype, pin_memory=True)
     x_host.copy_(x)
-    xh = x_host.numpy()
-    yh = y_host.numpy()
     native = plan._native_plan
-    if args.dtype == "c128":
-        host_apply = lambda: native.apply_into(xh, yh, 2**63 - 1)  # noqa: E731
-    else:
-        host_apply = lambda: native.apply_c64_into(xh, yh)  # noqa: E731
-    host_apply()
-    e2e_times = []
-    for _ in range(args.e2e_steps):
-        t0 = time.perf_counter()
-        host_apply()
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_local = statistics.median(e2e_times)
-    e2e_tensor = torch.tensor([e2e_local], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(e2e_tensor, op=dist.ReduceOp.MAX)
-    e2e_value = amp_terms * world / float(e2e_tensor.item())
+
+    def host_apply(xh: np.ndarray, yh: np.ndarray) -> None:
+        if args.dtype == "c128":
+            native.apply_into(xh, yh, 2**63 - 1)
+        else:
+            native.apply_c64_into(xh, yh)
+
+    def e2e_time(xh: np.ndarray, yh: np.ndarray) -> float:
+        host_apply(xh, yh)
+        times = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            host_apply(xh, yh)
+            times.append(time.perf_counter() - t0)
+        t = torch.tensor([statistics.median(times)], device="cuda", dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    x_page = np.array(x_host.numpy(), copy=True)
+    y_page = np.empty_like(x_page)
+    e2e_pageable_s = e2e_time(x_page, y_page)
+    e2e_pinned_s = e2e_time(x_host.numpy(), y_host.numpy())
+    del x_page, y_page
+    e2e_value = amp_terms * world / e2e_pageable_s
 
     # accuracy of this run's result on a row sample (rank 0), vs the oracle
     line: Dict[str, Any] = {}
@@ -872,19 +997,25 @@ def main() -> None:
         kern_ms = statistics.mean(kernel_ms)
         b_alg = dim * 2 * elem
         achieved = b_alg / (kern_ms / 1000.0) / 1e9
-        kernel_name = "k_tiled<3,double>" if args.dtype == "c128" else "k_tiled<3,float>"
+        kernel_name = "k_ring<double>" if args.dtype == "c128" else "k_ring<float>"
         traffic = _profile_traffic(kernel_name)
-        # The binding ceiling is the FMA pipe: F_alg = 2^n (2T + 8G) real flops
-        # (the +-w_k sums into D_m once per amplitude, one complex multiply-add
-        # per group), against this GPU's own FMA rate.
+        # Ceilings of k_ring.  Binding: shared-memory operand delivery -- per
+        # output row one operand per coset (groups whose inner masks agree on
+        # the thread bits share it) read by the consumer warps, plus one value
+        # per ring step written by the TMA engine -- against the device's own
+        # shared-memory rate.  Beside it: the FMA pipe, F_alg = 2^n (2T + 8G)
+        # real flops (the +-w_k sums into D_m once per amplitude, one complex
+        # multiply-add per group), and HBM (read x once, write y once).
         from tencirpauli_b200 import _native as native_mod
 
         fma_rate, _ = native_mod.probe_fma_rate("complex128" if args.dtype == "c128" else "complex64")
+        smem_rate, _ = native_mod.probe_smem_rate()
         G = plan.group_count
+        info = native.info
         f_alg = dim * (2 * T + 8 * G)
         f_ach = f_alg / (kern_ms / 1000.0)
-        smem_bytes = dim * G * elem  # one operand per (row, group) from shared memory
-        smem_peak = 128.0 * torch.cuda.get_device_properties(0).multi_processor_count * 1.965e9
+        smem_bytes = dim * (int(info.cosets) + int(info.ring_steps)) * elem
+        smem_ach = smem_bytes / (kern_ms / 1000.0)
         line = {
             "metric": METRIC,
             "value": value,
@@ -900,16 +1031,27 @@ def main() -> None:
             "data": "synthetic",
             "config": workload_config(args, op),
             "roofline": {
-                "bound": "fp64" if args.dtype == "c128" else "fp32",
-                "achieved": f_ach / 1e12,
-                "peak": fma_rate / 1e12,
-                "unit": "TFLOP/s",
-                "frac": f_ach / fma_rate,
+                "bound": "smem",
+                "achieved": smem_ach / 1e12,
+                "peak": smem_rate / 1e12,
+                "unit": "TB/s",
+                "frac": smem_ach / smem_rate,
                 "traffic": traffic,
-                "peak_source": "tcp_probe_fma_rate: FMA chains on every SM of this GPU, best of 5",
+                "peak_source": "tcp_probe_smem_rate: 16-byte shared-memory reads in the kernel's pattern on every SM "
+                "of this GPU, best of 5",
                 "kernel": kernel_name,
-                "flops_per_launch": f_alg,
                 "kernel_ms": kern_ms,
+                "smem_bytes_per_launch": smem_bytes,
+                "smem_units": f"2^{n} rows x ({int(info.cosets)} coset operands + {int(info.ring_steps)} tile fills) "
+                f"x {elem} B",
+                "fp": {
+                    "achieved": f_ach / 1e12,
+                    "peak": fma_rate / 1e12,
+                    "unit": "TFLOP/s",
+                    "frac": f_ach / fma_rate,
+                    "flops_per_launch": f_alg,
+                    "peak_source": "tcp_probe_fma_rate: FMA chains on every SM of this GPU, best of 5",
+                },
                 "hbm": {
                     "achieved": achieved,
                     "peak": peaks["hbm_gbs"],
@@ -919,19 +1061,16 @@ def main() -> None:
                     "peak_source": peaks["source"],
                     "traffic_gbs": (traffic / (kern_ms / 1000.0) / 1e9) if traffic else None,
                 },
-                "smem_operands": {
-                    "bytes_per_launch": smem_bytes,
-                    "achieved_tbs": smem_bytes / (kern_ms / 1000.0) / 1e12,
-                    "nominal_peak_tbs": smem_peak / 1e12,
-                    "frac": smem_bytes / (kern_ms / 1000.0) / smem_peak,
-                },
             },
             "e2e": {
                 "value": e2e_value,
                 "unit": UNIT,
                 "h2d_bytes_per_step": dim * elem,
                 "d2h_bytes_per_step": dim * elem,
-                "ms_per_step": 1000.0 * float(e2e_tensor.item()),
+                "ms_per_step": 1000.0 * e2e_pageable_s,
+                "host_buffers": "ordinary (pageable) NumPy arrays",
+                "pinned": {"value": amp_terms * world / e2e_pinned_s, "ms_per_step": 1000.0 * e2e_pinned_s,
+                           "host_buffers": "page-locked"},
             },
             "gpu_launches": args.steps,
             "clocks": clocks,
@@ -939,7 +1078,8 @@ def main() -> None:
             "plan": {
                 "groups": plan.group_count,
                 "tile_bits": int(native.info.tile_bits),
-                "steps": int(native.info.steps),
+                "ring_steps": int(native.info.ring_steps),
+                "cosets": int(native.info.cosets),
                 "outer_patterns": int(native.info.outer_patterns),
             },
         }

@@ -95,6 +95,8 @@ typedef struct tcp_mvp_plan_info_t {
     uint32_t log_threads;      /* log2 threads per tile (rows per thread = 2^(tile_bits - log_threads)) */
     uint64_t steps;            /* tile loads per output tile (outer patterns, split at 16 KiB of term data) */
     uint64_t outer_patterns;   /* distinct outer patterns d = x_mask >> tile_bits */
+    uint64_t ring_steps;       /* tile loads per output tile of the ring kernel (0: not used) */
+    uint64_t cosets;           /* operand loads per output tile of the ring kernel (groups sharing them) */
 } tcp_mvp_plan_info_t;
 
 /* Library version (TCP_ABI_VERSION) */
@@ -174,6 +176,11 @@ int tcp_mvp_apply_into_host_c64(const tcp_mvp_plan *plan, const float *state,
  */
 int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
                               uint64_t len, uint32_t nrhs, int dtype, void *stream);
+/* The same with d_result += H d_state instead of overwriting (no counterpart
+ * in the reference, whose apply_into always overwrites): the shard-exchange
+ * path adds every partner's contribution to its output shard this way. */
+int tcp_mvp_apply_add_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
+                             uint64_t len, uint32_t nrhs, int dtype, void *stream);
 
 /*
  * Batched MVP: many plans (Hamiltonians of uneven qubit and term counts), each

@@ -58,6 +58,7 @@ EXPORTED_SYMBOLS = (
     "tcp_mvp_apply_into_host",
     "tcp_mvp_apply_into_host_c64",
     "tcp_mvp_apply_into_device",
+    "tcp_mvp_apply_add_device",
     "tcp_mvp_apply_into_host_noalloc",
     "tcp_mvp_plan_device_status",
     "tcp_selftest_bounded_wait",
@@ -113,7 +114,7 @@ TCP_MATRIX_COO = 0
 TCP_MATRIX_CSR = 1
 
 # Every symbol include/tcp_probe.h declares.
-PROBE_SYMBOLS = ("tcp_probe_fma_rate",)
+PROBE_SYMBOLS = ("tcp_probe_fma_rate", "tcp_probe_smem_rate")
 
 
 class TcpU1PlanInfo(ctypes.Structure):
@@ -150,6 +151,8 @@ class TcpPlanInfo(ctypes.Structure):
         ("log_threads", ctypes.c_uint32),
         ("steps", ctypes.c_uint64),
         ("outer_patterns", ctypes.c_uint64),
+        ("ring_steps", ctypes.c_uint64),
+        ("cosets", ctypes.c_uint64),
     ]
 
 
@@ -189,6 +192,7 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mvp_apply_into_host.argtypes = [vp, f64p, u64, f64p, u64, u64]
         lib.tcp_mvp_apply_into_host_c64.argtypes = [vp, f32p, u64, f32p, u64]
         lib.tcp_mvp_apply_into_device.argtypes = [vp, vp, vp, u64, u32, i32, vp]
+        lib.tcp_mvp_apply_add_device.argtypes = [vp, vp, vp, u64, u32, i32, vp]
         lib.tcp_mvp_apply_into_host_noalloc.argtypes = [vp, f64p, u64, f64p, u64, vp]
         lib.tcp_mvp_plan_device_status.argtypes = [vp]
         lib.tcp_selftest_bounded_wait.argtypes = [vp, u64]
@@ -239,6 +243,8 @@ def load_library() -> ctypes.CDLL:
             getattr(lib, name).restype = i32
         lib.tcp_probe_fma_rate.argtypes = [i32, u32, f64p, f64p]
         lib.tcp_probe_fma_rate.restype = i32
+        lib.tcp_probe_smem_rate.argtypes = [u32, f64p, f64p]
+        lib.tcp_probe_smem_rate.restype = i32
         for name in SOLVER_SYMBOLS:
             if not name.endswith("_work_bytes"):
                 getattr(lib, name).restype = i32
@@ -485,12 +491,13 @@ class NativeMvpPlan:
         raise_for_status(status)
 
     # -- device apply -----------------------------------------------------
-    def apply_device(self, x: Any, y: Any, stream: Any = None) -> None:
+    def apply_device(self, x: Any, y: Any, stream: Any = None, accumulate: bool = False) -> None:
         """Apply to torch CUDA tensors of shape (dim,) or (nrhs, dim).
 
         complex128 tensors run the FP64 kernel, complex64 tensors the FP32
         Kahan kernel.  Asynchronous on ``stream`` (default: torch's current
-        stream on the plan's device).
+        stream on the plan's device).  ``accumulate`` adds H x to y
+        (``tcp_mvp_apply_add_device``) instead of overwriting it.
         """
         import torch
 
@@ -509,7 +516,8 @@ class NativeMvpPlan:
             stream = torch.cuda.current_stream(x.device)
         handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
         dtype = TCP_DTYPE_C128 if x.dtype == torch.complex128 else TCP_DTYPE_C64
-        status = self._lib.tcp_mvp_apply_into_device(
+        entry = self._lib.tcp_mvp_apply_add_device if accumulate else self._lib.tcp_mvp_apply_into_device
+        status = entry(
             self._handle,
             ctypes.c_void_p(x.data_ptr()),
             ctypes.c_void_p(y.data_ptr()),
@@ -863,4 +871,13 @@ def probe_fma_rate(dtype: str = "complex128", repeats: int = 5) -> Tuple[float, 
     raise_for_status(
         load_library().tcp_probe_fma_rate(code, repeats, _ptr(rate, ctypes.c_double), _ptr(ms, ctypes.c_double))
     )
+    return float(rate[0]), float(ms[0])
+
+
+def probe_smem_rate(repeats: int = 5) -> Tuple[float, float]:
+    """(bytes/s, best launch ms) that the device's shared memory delivers to
+    registers in the tiled kernels' access pattern (``tcp_probe_smem_rate``)."""
+    rate = np.zeros(1, np.float64)
+    ms = np.zeros(1, np.float64)
+    raise_for_status(load_library().tcp_probe_smem_rate(repeats, _ptr(rate, ctypes.c_double), _ptr(ms, ctypes.c_double)))
     return float(rate[0]), float(ms[0])

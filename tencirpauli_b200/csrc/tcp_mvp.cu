@@ -20,7 +20,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdlib>
+#include <thread>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     }
     C *yt = y + (tile << S);
-    if (PASSES && accumulate) {
+    if (accumulate) {
 #pragma unroll
         for (int j = 0; j < E; ++j) {
             C &out = yt[tid + (j << kLogThreads)];
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(kRingThreads, 1)
         }
     }
     C *yt = y + (tile << kTileBitsC128);
-    if (PASSES && accumulate) {
+    if (accumulate) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             C &out = yt[tid + (j << kLogThreads)];
@@ -461,7 +463,7 @@ __global__ void __launch_bounds__(kRingThreads, 1)
 // One thread per row; gathers straight from global memory.
 template <typename R>
 __global__ void k_rowwise(DevSchedule s, const typename Cx<R>::T *__restrict__ x,
-                          typename Cx<R>::T *__restrict__ y, uint64_t dim) {
+                          typename Cx<R>::T *__restrict__ y, uint64_t dim, uint32_t accumulate) {
     using C = typename Cx<R>::T;
     for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; r < dim;
          r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -478,7 +480,13 @@ __global__ void k_rowwise(DevSchedule s, const typename Cx<R>::T *__restrict__ x
             }
             acc.add_product(dre, dimv, v);
         }
-        y[r] = acc.value();
+        if (accumulate) {
+            const C v = acc.value();
+            y[r].x += v.x;
+            y[r].y += v.y;
+        } else {
+            y[r] = acc.value();
+        }
     }
 }
 
@@ -749,7 +757,7 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
                 accumulate ? 1u : 0u);
         } else {
             k_ring<R, false><<<static_cast<unsigned>(tiles), kRingThreads, smem, stream>>>(
-                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, 0u);
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, accumulate ? 1u : 0u);
         }
     } else if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
         int st = ensure_smem_attrs<R>(p->device);
@@ -762,14 +770,14 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
                 accumulate ? 1u : 0u);
         } else {
             k_tiled<LOGE, R, false><<<static_cast<unsigned>(tiles), kThreads, smem, stream>>>(
-                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, 0u);
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, accumulate ? 1u : 0u);
         }
     } else {
         const int threads = 256;
         uint64_t blocks = (p->dim + threads - 1) / threads;
         blocks = std::min<uint64_t>(blocks, 1u << 20);
         k_rowwise<R><<<static_cast<unsigned>(blocks), threads, 0, stream>>>(
-            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->dim);
+            ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->dim, accumulate ? 1u : 0u);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "MVP kernel launch");
@@ -785,6 +793,185 @@ int read_device_status(const tcp_mvp_plan *p) {
         if (h & kErrTimeout) return fail(TCP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
     }
     return TCP_OK;
+}
+
+// Host threads for the copies between a caller's ordinary (pageable) buffer
+// and the page-locked staging slots.  One copy at a time, split over the
+// workers and the calling thread; the pool lives until the process exits.
+class CopyPool {
+  public:
+    static CopyPool &get() {
+        static CopyPool *pool = new CopyPool(std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2)));
+        return *pool;
+    }
+    void copy(void *dst, const void *src, size_t bytes) {
+        std::lock_guard<std::mutex> call(call_mutex_);
+        {
+            std::lock_guard<std::mutex> lock(mutex_);
+            dst_ = static_cast<unsigned char *>(dst);
+            src_ = static_cast<const unsigned char *>(src);
+            bytes_ = bytes;
+            pending_ = workers_;
+            ++generation_;
+        }
+        start_.notify_all();
+        piece(workers_);
+        std::unique_lock<std::mutex> lock(mutex_);
+        finished_.wait(lock, [&] { return pending_ == 0; });
+    }
+
+  private:
+    explicit CopyPool(unsigned workers) : workers_(workers) {
+        for (unsigned w = 0; w < workers; ++w) std::thread([this, w] { run(w); }).detach();
+    }
+    void piece(unsigned index) {
+        const size_t parts = workers_ + 1;
+        const size_t per = ((bytes_ / parts) + 4095) & ~size_t(4095);
+        const size_t off = per * index;
+        if (off < bytes_) std::memcpy(dst_ + off, src_ + off, std::min(per, bytes_ - off));
+    }
+    void run(unsigned index) {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lock(mutex_);
+                start_.wait(lock, [&] { return generation_ != seen; });
+                seen = generation_;
+            }
+            piece(index);
+            std::lock_guard<std::mutex> lock(mutex_);
+            if (--pending_ == 0) finished_.notify_all();
+        }
+    }
+    unsigned workers_;
+    std::mutex call_mutex_, mutex_;
+    std::condition_variable start_, finished_;
+    unsigned char *dst_ = nullptr;
+    const unsigned char *src_ = nullptr;
+    size_t bytes_ = 0;
+    unsigned pending_ = 0;
+    uint64_t generation_ = 0;
+};
+
+// Page-locked host memory (cudaHostAlloc or cudaHostRegister) moves by DMA
+// without staging.
+bool page_locked(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Copies of one host apply.  Page-locked buffers go straight to the DMA
+// engine.  Ordinary buffers of at least two slots go through the staging
+// ring: the host threads fill a free slot while the DMA engine drains the
+// previous ones (input), or empty a slot whose DMA has landed while later
+// slots are in flight (output), so both directions stay asynchronous to the
+// kernels.
+struct HostCopies {
+    tcp::Staging *stage = nullptr;
+    bool stage_in = false, stage_out = false;
+    struct Out {
+        unsigned char *dst;
+        size_t len;
+        int slot;
+    };
+    std::vector<Out> inflight;  // output slots in flight, oldest first
+
+    unsigned char *slot_ptr(int slot) const { return stage->host + static_cast<size_t>(slot) * tcp::kStageSlotBytes; }
+    int next_slot() {
+        const int slot = static_cast<int>(stage->uses % tcp::kStageSlots);
+        ++stage->uses;
+        return slot;
+    }
+    int to_device(void *dst, const void *src, size_t len, cudaStream_t s) {
+        if (!stage_in) {
+            cudaError_t e = cudaMemcpyAsync(dst, src, len, cudaMemcpyHostToDevice, s);
+            return e == cudaSuccess ? TCP_OK : cuda_fail(e, "H2D copy");
+        }
+        for (size_t off = 0; off < len; off += tcp::kStageSlotBytes) {
+            const size_t n = std::min(tcp::kStageSlotBytes, len - off);
+            const int slot = next_slot();
+            cudaError_t e = cudaEventSynchronize(stage->ev[slot]);  // its previous DMA has finished
+            if (e != cudaSuccess) return cuda_fail(e, "staging slot");
+            CopyPool::get().copy(slot_ptr(slot), static_cast<const unsigned char *>(src) + off, n);
+            e = cudaMemcpyAsync(static_cast<unsigned char *>(dst) + off, slot_ptr(slot), n, cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(stage->ev[slot], s);
+            if (e != cudaSuccess) return cuda_fail(e, "staged H2D copy");
+        }
+        return TCP_OK;
+    }
+    int drain_one() {
+        const Out o = inflight.front();
+        inflight.erase(inflight.begin());
+        cudaError_t e = cudaEventSynchronize(stage->ev[o.slot]);
+        if (e != cudaSuccess) return cuda_fail(e, "staged D2H copy");
+        CopyPool::get().copy(o.dst, slot_ptr(o.slot), o.len);
+        return TCP_OK;
+    }
+    int to_host(void *dst, const void *src, size_t len, cudaStream_t s) {
+        if (!stage_out) {
+            cudaError_t e = cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToHost, s);
+            return e == cudaSuccess ? TCP_OK : cuda_fail(e, "D2H copy");
+        }
+        for (size_t off = 0; off < len; off += tcp::kStageSlotBytes) {
+            const size_t n = std::min(tcp::kStageSlotBytes, len - off);
+            if (inflight.size() == static_cast<size_t>(tcp::kStageSlots)) {
+                int st = drain_one();
+                if (st) return st;
+            }
+            const int slot = next_slot();
+            cudaError_t e = cudaEventSynchronize(stage->ev[slot]);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(slot_ptr(slot), static_cast<const unsigned char *>(src) + off, n,
+                                    cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaEventRecord(stage->ev[slot], s);
+            if (e != cudaSuccess) return cuda_fail(e, "staged D2H copy");
+            inflight.push_back({static_cast<unsigned char *>(dst) + off, n, slot});
+        }
+        return TCP_OK;
+    }
+    int finish() {
+        while (!inflight.empty()) {
+            int st = drain_one();
+            if (st) return st;
+        }
+        return TCP_OK;
+    }
+};
+
+int ensure_staging(tcp::Workspace &ws) {
+    if (ws.stage) return TCP_OK;
+    auto *stage = new tcp::Staging();
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&stage->host), tcp::kStageSlots * tcp::kStageSlotBytes,
+                                  cudaHostAllocPortable);
+    for (int k = 0; k < tcp::kStageSlots && e == cudaSuccess; ++k)
+        e = cudaEventCreateWithFlags(&stage->ev[k], cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+        // every slot starts free: its event has completed
+        for (int k = 0; k < tcp::kStageSlots && e == cudaSuccess; ++k) e = cudaEventRecord(stage->ev[k], nullptr);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        for (auto &ev : stage->ev)
+            if (ev) cudaEventDestroy(ev);
+        if (stage->host) cudaFreeHost(stage->host);
+        delete stage;
+        return fail(TCP_ERR_ALLOCATION, std::string("page-locked staging ring: ") + cudaGetErrorString(e));
+    }
+    ws.stage = stage;
+    return TCP_OK;
+}
+
+void release_staging(tcp::Staging *stage) {
+    if (!stage) return;
+    for (auto &ev : stage->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (stage->host) cudaFreeHost(stage->host);
+    delete stage;
 }
 
 template <typename R>
@@ -819,20 +1006,36 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         std::lock_guard<std::mutex> lock(plan->ws_mutex);
         plan->ws_all.push_back(ws);
     }
-    cudaStream_t stream = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    HostCopies copies;
     int status = TCP_OK;
+    const bool large = bytes >= 2 * tcp::kStageSlotBytes;
+    copies.stage_in = large && !page_locked(state);
+    copies.stage_out = large && !page_locked(result);
+    if (copies.stage_in || copies.stage_out) {
+        if (ensure_staging(ws) == TCP_OK) {
+            std::lock_guard<std::mutex> lock(plan->ws_mutex);
+            for (auto &w : plan->ws_all)
+                if (w.x == ws.x) w.stage = ws.stage;
+            copies.stage = ws.stage;
+        } else {
+            // no page-locked memory to stage through: plain (synchronous) copies
+            copies.stage_in = copies.stage_out = false;
+        }
+    }
+    cudaStream_t stream = nullptr;
+    cudaError_t e = status ? cudaSuccess : cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) status = cuda_fail(e, "cudaStreamCreate");
     // Large tiled applies overlap both copies with the kernel.
     //  * Input: the state goes in as kPassChunks equal parts on its own
     //    stream.  Pass k waits for part k only and runs the steps whose source
-    //    tiles lie in it (k_tiled's `pass`), adding to y after the first, so
-    //    the copy of parts 1.. overlaps the earlier passes.
+    //    tiles lie in it (the kernels' `pass`), adding to y after the first,
+    //    so the copy of parts 1.. overlaps the earlier passes.
     //  * Output: the last pass runs in kHostChunks launches over consecutive
     //    output tiles; a third stream copies each finished chunk of y to the
     //    host while the next chunk computes.
-    // All copies and launches are queued before the host waits on any of
-    // them.  Smaller applies copy, launch once and copy back on one stream.
+    // Every launch is queued right after the copy it waits for; ordinary
+    // (pageable) buffers move through the staging ring (HostCopies).  Smaller
+    // applies copy, launch once and copy back on one stream.
     const uint64_t tiles = tiled_tiles<R>(plan, ws.x);
     const uint64_t chunks = tiles >= kHostChunkTiles ? kHostChunks : 1;
     const bool passes = chunks > 1 && has_passes(plan, ws.x);
@@ -848,28 +1051,21 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
             e = cudaEventCreateWithFlags(&landed[k], cudaEventDisableTiming);
         if (e != cudaSuccess) status = cuda_fail(e, "creating the copy streams");
     }
-    if (!status && passes) {
-        const size_t part = bytes / kParts;
-        for (int k = 0; k < kParts && !status; ++k) {
-            e = cudaMemcpyAsync(static_cast<unsigned char *>(ws.x) + k * part,
-                                reinterpret_cast<const unsigned char *>(state) + k * part, part,
-                                cudaMemcpyHostToDevice, in_stream);
-            if (e == cudaSuccess) e = cudaEventRecord(landed[k], in_stream);
-            if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
-        }
-    } else if (!status) {
-        e = cudaMemcpyAsync(ws.x, state, bytes, cudaMemcpyHostToDevice, stream);
-        if (e != cudaSuccess) status = cuda_fail(e, "H2D copy");
-    }
     if (!status && chunks > 1) {
-        for (int k = 0; passes && k < kParts - 1 && !status; ++k) {
-            e = cudaStreamWaitEvent(stream, landed[k], 0);
-            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
-            if (!status) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
-        }
-        if (!status && passes) {
-            e = cudaStreamWaitEvent(stream, landed[kParts - 1], 0);
-            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
+        if (passes) {
+            const size_t part = bytes / kParts;
+            for (int k = 0; k < kParts && !status; ++k) {
+                status = copies.to_device(static_cast<unsigned char *>(ws.x) + k * part,
+                                          reinterpret_cast<const unsigned char *>(state) + k * part, part, in_stream);
+                if (!status) {
+                    e = cudaEventRecord(landed[k], in_stream);
+                    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, landed[k], 0);
+                    if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
+                }
+                if (!status && k < kParts - 1) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
+            }
+        } else {
+            status = copies.to_device(ws.x, state, bytes, stream);
         }
         const uint64_t per = tiles / chunks;
         for (uint64_t c = 0; c < chunks && !status; ++c) {
@@ -887,19 +1083,17 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
             const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
             const size_t off = t0 * rows_per_tile * row_bytes, len = nt * rows_per_tile * row_bytes;
             e = cudaStreamWaitEvent(copy_stream, done[c], 0);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(reinterpret_cast<unsigned char *>(result) + off,
-                                    static_cast<const unsigned char *>(ws.y) + off, len, cudaMemcpyDeviceToHost,
-                                    copy_stream);
-            if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
+            if (e != cudaSuccess) status = cuda_fail(e, "waiting for an output chunk");
+            if (!status)
+                status = copies.to_host(reinterpret_cast<unsigned char *>(result) + off,
+                                        static_cast<const unsigned char *>(ws.y) + off, len, copy_stream);
         }
     } else if (!status) {
-        status = launch_one<R>(plan, ws.x, ws.y, stream);
-        if (!status) {
-            e = cudaMemcpyAsync(result, ws.y, bytes, cudaMemcpyDeviceToHost, stream);
-            if (e != cudaSuccess) status = cuda_fail(e, "D2H copy");
-        }
+        status = copies.to_device(ws.x, state, bytes, stream);
+        if (!status) status = launch_one<R>(plan, ws.x, ws.y, stream);
+        if (!status) status = copies.to_host(result, ws.y, bytes, stream);
     }
+    if (!status) status = copies.finish();
     for (cudaStream_t side : {in_stream, copy_stream}) {
         if (!side) continue;
         e = cudaStreamSynchronize(side);
@@ -914,6 +1108,11 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         e = cudaStreamSynchronize(stream);
         if (!status && e != cudaSuccess) status = cuda_fail(e, "stream synchronize");
         cudaStreamDestroy(stream);
+    }
+    if (ws.stage) {
+        // staging events may still name copies that an error path left
+        // queued; the streams are synchronised above, so every slot is free
+        ws.stage->uses = 0;
     }
     if (!status) status = read_device_status(plan);
     {
@@ -997,6 +1196,7 @@ extern "C" int tcp_mvp_plan_destroy(tcp_mvp_plan *plan) {
     for (auto &w : plan->ws_all) {
         cudaFree(w.x);
         cudaFree(w.y);
+        release_staging(w.stage);
     }
     if (plan->dev_block) cudaFree(plan->dev_block);
     if (prev >= 0 && prev != plan->device) cudaSetDevice(prev);
@@ -1019,6 +1219,8 @@ extern "C" int tcp_mvp_plan_info(const tcp_mvp_plan *plan, tcp_mvp_plan_info_t *
     info->log_threads = plan->sched.host.log_threads;
     info->steps = plan->sched.host.step_info.size() / 4;
     info->outer_patterns = plan->sched.host.distinct_outer;
+    info->ring_steps = plan->sched.ring.step_info.size() / 4;
+    info->cosets = plan->sched.ring.cosets;
     return TCP_OK;
 }
 
@@ -1033,8 +1235,9 @@ extern "C" int tcp_mvp_apply_into_host_c64(const tcp_mvp_plan *plan, const float
     return apply_host<float>(plan, state, state_len, result, result_len);
 }
 
-extern "C" int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
-                                         uint64_t len, uint32_t nrhs, int dtype, void *stream) {
+namespace {
+int apply_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result, uint64_t len, uint32_t nrhs,
+                 int dtype, void *stream, bool accumulate) {
     int st = check_plan(plan);
     if (st) return st;
     if (len != plan->dim) return length_error(plan->dim, len);
@@ -1048,10 +1251,22 @@ extern "C" int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d
     for (uint32_t v = 0; v < nrhs; ++v) {
         const void *x = static_cast<const unsigned char *>(d_state) + static_cast<size_t>(v) * len * elem;
         void *y = static_cast<unsigned char *>(d_result) + static_cast<size_t>(v) * len * elem;
-        st = dtype == TCP_DTYPE_C128 ? launch_one<double>(plan, x, y, s) : launch_one<float>(plan, x, y, s);
+        st = dtype == TCP_DTYPE_C128 ? launch_one<double>(plan, x, y, s, 0, 0, -1, accumulate)
+                                     : launch_one<float>(plan, x, y, s, 0, 0, -1, accumulate);
         if (st) return st;
     }
     return TCP_OK;
+}
+}  // namespace
+
+extern "C" int tcp_mvp_apply_into_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result,
+                                         uint64_t len, uint32_t nrhs, int dtype, void *stream) {
+    return apply_device(plan, d_state, d_result, len, nrhs, dtype, stream, false);
+}
+
+extern "C" int tcp_mvp_apply_add_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result, uint64_t len,
+                                        uint32_t nrhs, int dtype, void *stream) {
+    return apply_device(plan, d_state, d_result, len, nrhs, dtype, stream, true);
 }
 
 extern "C" int tcp_mvp_plan_device_status(const tcp_mvp_plan *plan) {
@@ -1226,7 +1441,7 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     } else {
         const int threads = 256;
         const uint64_t blocks = (plan->dim + threads - 1) / threads;
-        k_rowwise<double><<<static_cast<unsigned>(blocks), threads, 0, s>>>(ds.dev, dx, dy, plan->dim);
+        k_rowwise<double><<<static_cast<unsigned>(blocks), threads, 0, s>>>(ds.dev, dx, dy, plan->dim, 0u);
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "MVP kernel launch");

@@ -17,10 +17,23 @@ struct DeviceSchedule {
     tcpdev::DevSchedule dev{};
 };
 
+// Page-locked staging ring of a host apply whose caller's buffers are
+// ordinary (pageable) memory: kStageSlots slots of kStageSlotBytes; slot use u
+// goes to slot u % kStageSlots, and ev[slot] marks the end of its last DMA.
+constexpr int kStageSlots = 4;
+constexpr size_t kStageSlotBytes = size_t(32) << 20;
+
+struct Staging {
+    unsigned char *host = nullptr;
+    cudaEvent_t ev[kStageSlots] = {};
+    uint64_t uses = 0;
+};
+
 struct Workspace {
     void *x = nullptr;
     void *y = nullptr;
     size_t bytes = 0;
+    Staging *stage = nullptr;  // allocated on the first pageable apply
 };
 
 int cuda_fail(cudaError_t e, const char *what);

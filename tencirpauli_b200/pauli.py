@@ -381,9 +381,10 @@ class NativeMVPPlan(NativeMvpFacade):
         return int(self._execution.group_count)
 
     # -- device-resident extensions (no host copies) ----------------------------
-    def apply_device(self, x: Any, y: Any, stream: Any = None) -> None:
-        """y <- H x for torch CUDA tensors (complex128: FP64, complex64: FP32 Kahan)."""
-        self._execution.apply_device(x, y, stream)
+    def apply_device(self, x: Any, y: Any, stream: Any = None, accumulate: bool = False) -> None:
+        """y <- H x (or y += H x with ``accumulate``) for torch CUDA tensors
+        (complex128: FP64, complex64: FP32 Kahan)."""
+        self._execution.apply_device(x, y, stream, accumulate)
 
     def diagonal_device(self, out: Any, stream: Any = None) -> None:
         self._execution.diagonal_device(out, stream)

@@ -16,10 +16,12 @@ those of the partner shard) -- the sign rule of
 Every rank takes the same exchange steps in the same order: for each nonzero
 pattern d (ascending), one pairwise send/receive with rank r ^ d through
 ``torch.distributed`` (NCCL on GPUs, gloo on CPU), then one local apply of
-H_d(r) to the received shard, accumulated into y.  The pattern d = 0 is
-applied to the local shard without communication.  Transfers go into a
-receive buffer in the rank's own memory and the local kernels read only local
-memory.
+H_d(r) to the received shard, added into y by the kernel itself
+(``tcp_mvp_apply_add_device``).  Two receive buffers alternate, and the
+exchange of pattern d+1 is posted before the apply of pattern d, so the
+transfer overlaps the compute.  The pattern d = 0 is applied to the local
+shard without communication.  Transfers go into receive buffers in the
+rank's own memory and the local kernels read only local memory.
 """
 
 from __future__ import annotations
@@ -115,24 +117,31 @@ class ShardedMVP:
         self.patterns = sorted(set(d for d in range(1, self.world) if any(pt.pattern == d for pt in self.parts)))
 
     def _device_apply(self, part: ShardTerms, x: Any, y: Any, accumulate: bool) -> None:
-        import torch
-
         plan = self._plans.get(part.pattern)
         if plan is None:
             low = PauliOperator.from_code_arrays(part.codes, part.coefficients) if len(part.coefficients) else PauliOperator.empty(self.local_qubits)
             plan = low.native_mvp_plan()
             self._plans[part.pattern] = plan
-        if accumulate:
-            tmp = torch.empty_like(y)
-            plan.apply_device(x, tmp)
-            y += tmp
-        else:
-            plan.apply_device(x, y)
+        plan.apply_device(x, y, accumulate=accumulate)
 
-    def apply(self, x: Any, y: Any, recv: Optional[Any] = None) -> None:
-        """y_r = sum_d H_d(r) x_{r ^ d}; x, y are this rank's shards."""
+    def receive_buffers(self, like: Any) -> List[Any]:
+        """The receive buffers that ``apply`` alternates between (two when
+        there are at least two exchange steps)."""
         import torch
 
+        return [torch.empty_like(like) for _ in range(min(2, len(self.patterns)))]
+
+    def _post(self, d: int, x: Any, buf: Any) -> List[Any]:
+        partner = self.rank ^ d
+        ops = [
+            self.dist.P2POp(self.dist.isend, x, partner, group=self.group),
+            self.dist.P2POp(self.dist.irecv, buf, partner, group=self.group),
+        ]
+        return self.dist.batch_isend_irecv(ops)
+
+    def apply(self, x: Any, y: Any, recv: Optional[Any] = None) -> None:
+        """y_r = sum_d H_d(r) x_{r ^ d}; x, y are this rank's shards.  ``recv``
+        is one buffer or a list of buffers shaped like x (default: fresh ones)."""
         if x.shape[-1] != self.shard_len or y.shape != x.shape:
             raise ValueError(f"shards must have length {self.shard_len}")
         by_pattern = {pt.pattern: pt for pt in self.parts}
@@ -141,18 +150,27 @@ class ShardedMVP:
             self.apply_fn(local, x, y, False)
         else:
             y.zero_()
+        if not self.patterns:
+            return
         if recv is None:
-            recv = torch.empty_like(x)
-        for d in self.patterns:
-            partner = self.rank ^ d
-            ops = [
-                self.dist.P2POp(self.dist.isend, x, partner, group=self.group),
-                self.dist.P2POp(self.dist.irecv, recv, partner, group=self.group),
-            ]
+            bufs = self.receive_buffers(x)
+        else:
+            bufs = list(recv) if isinstance(recv, (list, tuple)) else [recv]
+        pending = self._post(self.patterns[0], x, bufs[0])
+        for i, d in enumerate(self.patterns):
+            reqs, buf = pending, bufs[i % len(bufs)]
+            following = None
+            if i + 1 < len(self.patterns) and len(bufs) > 1:
+                # the next exchange runs while this pattern is applied; its
+                # buffer was read by the apply before the previous one, which
+                # is ordered before it on the device
+                following = self._post(self.patterns[i + 1], x, bufs[(i + 1) % len(bufs)])
             # A partner that left makes this wait end with an error after the
             # timeout instead of blocking the rank for good.
-            for req in self.dist.batch_isend_irecv(ops):
+            for req in reqs:
                 req.wait(self.timeout)
             part = by_pattern.get(d)
             if part is not None:
-                self.apply_fn(part, recv, y, True)
+                self.apply_fn(part, buf, y, True)
+            if i + 1 < len(self.patterns):
+                pending = following if following is not None else self._post(self.patterns[i + 1], x, bufs[0])
