@@ -89,6 +89,16 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// Non-blocking test of an mbarrier phase.
+__device__ __forceinline__ uint32_t mbar_test_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok;
+}
 __device__ __forceinline__ uint32_t mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -227,5 +237,57 @@ template <> struct Acc<float> {
     __device__ __forceinline__ float2 value() const { return make_float2(re, im); }
 };
 
+// Row accumulator of the ring kernel.  FP64: the plain Acc.  FP32: (re, im)
+// pairs packed in 64-bit registers and updated with the paired FP32
+// instructions of sm_100 (fma/add/sub .rn.f32x2: each lane rounds exactly as
+// the scalar instruction), so one instruction serves both components.  Two
+// running partial sums -- p for real weights (w x) and q for imaginary
+// weights (w x, whose contribution is i q) -- take the same instruction form;
+// compensate() folds p + i q into the Kahan-compensated row sum.
+template <typename R> struct RingAcc;
+template <> struct RingAcc<double> : Acc<double> {};
+
+__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(uint64_t v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return make_float2(lo, hi);
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+template <> struct RingAcc<float> {
+    uint64_t s = 0, c = 0;  // Kahan sum and compensation, (re, im)
+    uint64_t p = 0, q = 0;  // running partial sums of real / imaginary weights
+    __device__ __forceinline__ void add_real(float w, float2 v) { p = fma2(pack2(w, w), pack2(v.x, v.y), p); }
+    __device__ __forceinline__ void add_imag(float w, float2 v) { q = fma2(pack2(w, w), pack2(v.x, v.y), q); }
+    __device__ __forceinline__ void compensate() {
+        const float2 qq = unpack2(q);
+        const uint64_t term = add2(p, pack2(-qq.y, qq.x));  // p + i q
+        const uint64_t yv = sub2(term, c);
+        const uint64_t tv = add2(s, yv);
+        c = sub2(sub2(tv, s), yv);
+        s = tv;
+        p = q = 0;
+    }
+    __device__ __forceinline__ float2 value() const { return unpack2(s); }
+};
 
 }  // namespace tcpdev

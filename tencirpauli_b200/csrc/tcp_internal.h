@@ -84,7 +84,10 @@ struct Schedule {
 // Block layout (16-byte units):
 //   header    {ncosets, ngroups, terms offset / 16, 0}
 //   cosets    {m_lo, jh_load, groups in the coset, 0} each
-//   groups    u32 each: a | nterms << 4, padded to 16 bytes
+//   groups    u32 each: a | nterms << 4, padded to 16 bytes; a group's
+//             records come in four runs (real weights with one sign for all
+//             rows of a thread, real with a row pattern, then the same for
+//             imaginary weights)
 //   terms     16 bytes each: meta = zlo | pattern << 9 | imag << 17, zt32 =
 //             z >> S (low 32 bits), then the folded weight: one f64
 //             (complex128 blocks) or one f32 + 4 pad bytes (complex64 blocks).

@@ -234,24 +234,41 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ------------------------------- ring kernel --------------------------------
-// k_ring: the tiled MVP with a warp-specialised ring of source tiles.
-//  * One producer warp (its lane 0) streams the steps of the output tile: it
-//    waits until the consumers have released a stage ("empty" mbarrier), then
-//    has the TMA bulk-copy engine fill that stage with the step's source tile
-//    (tile ^ d) and its block ("full" mbarrier with the byte count).
-//  * Sixteen consumer warps own the tile's 4096 rows (thread t: rows
+// k_ring: the tiled MVP with a ring of source tiles.
+//  * Sixteen warps own the output tile's 4096 rows (thread t: rows
 //    t + j * 512, j = 0..7) and keep their sums in registers.  Per step they
-//    wait for the stage, walk its cosets -- one row-ordered load of 8 source
-//    values per coset -- and apply every group of the coset through a
-//    compile-time register permutation a (row j reads loaded value j ^ a).
-//    Then each warp releases the stage with one arrive.  No CTA-wide barrier
-//    runs after set-up, so warps drift apart by up to the ring depth.
+//    wait for its stage ("full" mbarrier), walk its cosets -- one row-ordered
+//    load of 8 source values per coset -- and apply every group of the coset
+//    through a compile-time register permutation a (row j reads loaded value
+//    j ^ a).  Then each warp releases the stage with one arrive ("empty").
+//  * Thread 0 is also the producer: whenever a stage is released by every
+//    warp it has the TMA bulk-copy engine refill it with a later step's
+//    source tile (tile ^ d) and block.  It only tests the empty barriers
+//    (never waits on them), at each step and while its own warp waits for
+//    data, so no warp is set aside for issuing copies and no CTA-wide barrier
+//    runs after set-up: warps drift apart by up to the ring depth.
 //  * Every wait is bounded (2 s) and also ends when another thread raised the
-//    CTA's abort word; the kernel then records kErrTimeout.  The producer
-//    always waits (bounded) for the last copy it issued into each stage before
-//    it exits, so no copy is left writing into a finished block's memory.
-constexpr int kRingConsumerWarps = kThreads / 32;
-constexpr int kRingThreads = kThreads + 32;
+//    CTA's abort word; the kernel then records kErrTimeout, and thread 0
+//    waits (bounded) for the last fill of every stage before the block exits,
+//    so no copy is left writing into a finished block's memory.
+constexpr uint32_t kRingWarps = kThreads / 32;  // warps that own the tile's rows
+constexpr uint32_t kRingCompensateGroups = 8;  // FP32: groups per Kahan fold
+
+// Who refills the ring.  complex128: a dedicated producer warp waits on the
+// stages' "empty" barriers and issues the fills (measured faster for FP64,
+// whose row warps fit the 96 registers a 544-thread block leaves them).
+// complex64: no extra warp -- the row warp that releases a stage last issues
+// its refill -- so the 512 threads keep 128 registers for the paired FP32
+// accumulators.
+template <typename R> struct RingShape;
+template <> struct RingShape<double> {
+    static constexpr bool kProducerWarp = true;
+    static constexpr int kThreadsPerCta = kThreads + 32;
+};
+template <> struct RingShape<float> {
+    static constexpr bool kProducerWarp = false;
+    static constexpr int kThreadsPerCta = kThreads;
+};
 
 template <typename R> struct RingDepth;
 template <> struct RingDepth<double> { static constexpr uint32_t K = 3; };  // 3 x (64 + 8) KiB
@@ -286,7 +303,7 @@ template <> __device__ __forceinline__ float ring_weight<float>(uint4 rec) { ret
 // bits because t < 512.
 template <int A, typename R>
 __device__ __forceinline__ void ring_term(uint4 rec, uint32_t tid, uint32_t tile32,
-                                          const typename Cx<R>::T (&xv)[8], Acc<R> (&acc)[8]) {
+                                          const typename Cx<R>::T (&xv)[8], RingAcc<R> (&acc)[8]) {
     const uint32_t meta = rec.x;
     const uint32_t base = __popc((meta & tid) ^ (rec.y & tile32)) & 1u;
     const uint32_t pattern = (meta >> 9) & 0xffu;
@@ -313,26 +330,56 @@ __device__ __forceinline__ void ring_term(uint4 rec, uint32_t tid, uint32_t tile
     }
 }
 
+// The `nt` records of one group, two per iteration so that the integer work of
+// one overlaps the multiply-adds of the other.
 template <int A, typename R>
 __device__ __forceinline__ void ring_group(const uint4 *__restrict__ trm, uint32_t nt, uint32_t tid, uint32_t tile32,
-                                           const typename Cx<R>::T (&xv)[8], Acc<R> (&acc)[8]) {
-    for (uint32_t k = 0; k < nt; ++k) ring_term<A, R>(trm[k], tid, tile32, xv, acc);
+                                           const typename Cx<R>::T (&xv)[8], RingAcc<R> (&acc)[8]) {
+    uint32_t k = 0;
+    for (; k + 2u <= nt; k += 2u) {
+        const uint4 r0 = trm[k], r1 = trm[k + 1];
+        ring_term<A, R>(r0, tid, tile32, xv, acc);
+        ring_term<A, R>(r1, tid, tile32, xv, acc);
+    }
+    if (k < nt) ring_term<A, R>(trm[k], tid, tile32, xv, acc);
+}
+
+// Issue the fill of ring step `i` (source tile and block) into its stage.
+template <typename R>
+__device__ __forceinline__ void ring_fill(const DevSchedule &s, const typename Cx<R>::T *__restrict__ x,
+                                          uint64_t tile, const uint4 *__restrict__ info, uint32_t i,
+                                          unsigned char *smem, uint64_t *full) {
+    constexpr uint32_t K = RingDepth<R>::K;
+    constexpr uint32_t TILE_BYTES = ring_tile_bytes<R>();
+    const uint32_t st = i % K;
+    const uint4 in = __ldg(&info[i]);
+    const uint64_t d = static_cast<uint64_t>(in.x) | (static_cast<uint64_t>(in.y) << 32);
+    const uint32_t blk_bytes = in.w * 16u;
+    unsigned char *dst = smem + st * ring_stage_bytes<R>();
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&full[st], TILE_BYTES + blk_bytes);
+    bulk_copy_g2s(dst, x + ((tile ^ d) << kTileBitsC128), TILE_BYTES, &full[st]);
+    bulk_copy_g2s(dst + TILE_BYTES, ring_blocks<R>(s) + static_cast<size_t>(in.z) * 16u, blk_bytes, &full[st]);
 }
 
 template <typename R, bool PASSES>
-__global__ void __launch_bounds__(kRingThreads, 1)
+__global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
     k_ring(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
            int *__restrict__ err, uint64_t tile0, uint32_t pass, uint32_t accumulate) {
     using C = typename Cx<R>::T;
     constexpr uint32_t K = RingDepth<R>::K;
     constexpr uint32_t TILE_BYTES = ring_tile_bytes<R>();
     constexpr uint32_t STAGE = ring_stage_bytes<R>();
+    constexpr bool kProducerWarp = RingShape<R>::kProducerWarp;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[K];
     __shared__ __align__(8) uint64_t empty[K];
+    __shared__ uint32_t released[K];
+    __shared__ uint32_t issued_end;
     __shared__ int abort_word;
 
     const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
     const uint64_t tile = tile0 + blockIdx.x;
     uint32_t step0 = 0, nsteps = s.ring_steps;
     if constexpr (PASSES) {
@@ -348,56 +395,63 @@ __global__ void __launch_bounds__(kRingThreads, 1)
         step0 = b0;
         nsteps = b1 - b0;
     }
+    const uint4 *info = s.ring_info + step0;
     if (tid == 0) {
 #pragma unroll
         for (uint32_t k = 0; k < K; ++k) {
             mbar_init(&full[k], 1);
-            mbar_init(&empty[k], kRingConsumerWarps);
+            mbar_init(&empty[k], kRingWarps);
+            released[k] = 0;
         }
         abort_word = 0;
         fence_mbar_init();
+        if constexpr (!kProducerWarp) {
+            const uint32_t first = nsteps < K ? nsteps : K;
+            for (uint32_t i = 0; i < first; ++i) ring_fill<R>(s, x, tile, info, i, smem_raw, full);
+            issued_end = first;
+        }
     }
     __syncthreads();
     volatile int *abort_flag = &abort_word;
 
-    if (tid >= static_cast<uint32_t>(kThreads)) {
-        // ---------------- producer warp (lane 0 issues) ----------------
-        if (tid != static_cast<uint32_t>(kThreads)) return;
-        const uint4 *info = s.ring_info + step0;
-        const unsigned char *blocks = ring_blocks<R>(s);
-        uint32_t issued = 0;
-        for (uint32_t st = 0; st < nsteps; ++st) {
-            const uint32_t stage = st % K;
-            if (st >= K && !mbar_wait_or_abort(&empty[stage], ((st / K) - 1u) & 1u, abort_flag)) {
-                atomicOr(err, kErrTimeout);
-                *abort_flag = 1;
-                break;
+    if constexpr (kProducerWarp) {
+        if (tid >= kRingWarps * 32u) {
+            // ---------------- producer warp (lane 0 issues) ----------------
+            if (tid != kRingWarps * 32u) return;
+            uint32_t issued = 0;
+            for (uint32_t st = 0; st < nsteps; ++st) {
+                if (st >= K && !mbar_wait_or_abort(&empty[st % K], ((st / K) - 1u) & 1u, abort_flag)) {
+                    atomicOr(err, kErrTimeout);
+                    *abort_flag = 1;
+                    break;
+                }
+                ring_fill<R>(s, x, tile, info, st, smem_raw, full);
+                issued = st + 1;
             }
-            const uint4 in = __ldg(&info[st]);
-            const uint64_t d = static_cast<uint64_t>(in.x) | (static_cast<uint64_t>(in.y) << 32);
-            const uint32_t blk_bytes = in.w * 16u;
-            unsigned char *dst = smem_raw + stage * STAGE;
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&full[stage], TILE_BYTES + blk_bytes);
-            bulk_copy_g2s(dst, x + ((tile ^ d) << kTileBitsC128), TILE_BYTES, &full[stage]);
-            bulk_copy_g2s(dst + TILE_BYTES, blocks + static_cast<size_t>(in.z) * 16u, blk_bytes, &full[stage]);
-            issued = st + 1;
+            // the last fill issued into each stage has landed before this returns
+            for (uint32_t i = issued > K ? issued - K : 0u; i < issued; ++i)
+                mbar_wait_bounded(&full[i % K], (i / K) & 1u);
+            return;
         }
-        // the last copy issued into each stage has landed before this returns
-        for (uint32_t st = issued > K ? issued - K : 0u; st < issued; ++st) mbar_wait_bounded(&full[st % K], (st / K) & 1u);
-        return;
     }
 
-    // ---------------- consumer warps ----------------
+    // ---------------- row warps ----------------
     const uint32_t tile32 = static_cast<uint32_t>(tile);
-    Acc<R> acc[8];
-    uint32_t stage = 0, phase = 0;
+    RingAcc<R> acc[8];
+    uint32_t stage = 0, phase = 0, since = 0;
     for (uint32_t st = 0; st < nsteps; ++st) {
         const bool landed = mbar_wait_or_abort(&full[stage], phase, abort_flag);
         if (__any_sync(0xffffffffu, !landed)) {
-            if ((tid & 31u) == 0u) {
+            if (lane == 0u) {
                 atomicOr(err, kErrTimeout);
                 *abort_flag = 1;
+                if constexpr (!kProducerWarp) {
+                    // every fill issued so far has landed (bounded) before
+                    // the block may exit
+                    const uint32_t end = *reinterpret_cast<volatile uint32_t *>(&issued_end);
+                    for (uint32_t i = end > K ? end - K : 0u; i < end; ++i)
+                        mbar_wait_bounded(&full[i % K], (i / K) & 1u);
+                }
             }
             return;
         }
@@ -428,23 +482,44 @@ __global__ void __launch_bounds__(kRingThreads, 1)
                 default: ring_group<7, R>(trm, nt, tid, tile32, xv, acc); break;
                 }
                 trm += nt;
-                // FP32: fold the running group sum into the compensated row
-                // sum every kCompensateGroups groups
-                if (((g + 1) % kCompensateGroups) == 0u) {
+                // FP32: fold the running partial sums into the compensated
+                // row sum every kRingCompensateGroups groups (counted across
+                // steps)
+                if constexpr (sizeof(R) == 4) {
+                    if (++since == kRingCompensateGroups) {
+                        since = 0;
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) acc[j].compensate();
+                        for (int j = 0; j < 8; ++j) acc[j].compensate();
+                    }
                 }
             }
         }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j].compensate();
         __syncwarp();
-        if ((tid & 31u) == 0u) mbar_arrive(&empty[stage]);
+        if (lane == 0u) {
+            if constexpr (kProducerWarp) {
+                mbar_arrive(&empty[stage]);
+            } else {
+                // The warp that releases the stage last refills it with step
+                // st + K: its reads, and every other warp's, are ordered
+                // before the counter update (fence), and the refill after it.
+                __threadfence_block();
+                if (atomicAdd(&released[stage], 1u) == kRingWarps - 1u) {
+                    released[stage] = 0u;
+                    __threadfence_block();
+                    if (st + K < nsteps) {
+                        ring_fill<R>(s, x, tile, info, st + K, smem_raw, full);
+                        atomicMax(&issued_end, st + K + 1u);
+                    }
+                }
+            }
+        }
         if (++stage == K) {
             stage = 0;
             phase ^= 1u;
         }
     }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j].compensate();
     C *yt = y + (tile << kTileBitsC128);
     if (accumulate) {
 #pragma unroll
@@ -752,11 +827,11 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
         const uint64_t tiles = ntiles ? ntiles : (p->dim >> kTileBitsC128) - tile0;
         const size_t smem = ring_smem_bytes<R>();
         if (pass >= 0) {
-            k_ring<R, true><<<static_cast<unsigned>(tiles), kRingThreads, smem, stream>>>(
+            k_ring<R, true><<<static_cast<unsigned>(tiles), RingShape<R>::kThreadsPerCta, smem, stream>>>(
                 ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, static_cast<uint32_t>(pass),
                 accumulate ? 1u : 0u);
         } else {
-            k_ring<R, false><<<static_cast<unsigned>(tiles), kRingThreads, smem, stream>>>(
+            k_ring<R, false><<<static_cast<unsigned>(tiles), RingShape<R>::kThreadsPerCta, smem, stream>>>(
                 ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, accumulate ? 1u : 0u);
         }
     } else if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
@@ -1432,7 +1507,7 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     const tcp::DeviceSchedule &ds = plan->sched;
     const uint32_t S = kTileBitsC128;
     if (ring_ok(plan, dx)) {
-        k_ring<double, false><<<static_cast<unsigned>(plan->dim >> S), kRingThreads, ring_smem_bytes<double>(), s>>>(
+        k_ring<double, false><<<static_cast<unsigned>(plan->dim >> S), RingShape<double>::kThreadsPerCta, ring_smem_bytes<double>(), s>>>(
             ds.dev, dx, dy, d_status, 0, 0u, 0u);
     } else if (plan->nqubits >= S && ds.host.tile_bits == S) {
         const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();

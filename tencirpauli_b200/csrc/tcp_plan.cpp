@@ -1,6 +1,7 @@
 // Host side of libtcpmvp.so: error slot, canonicalization, term compilation and
 // the tile schedule.  Pure C++ (no CUDA); compiled by nvcc with the kernels.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdlib>
@@ -295,6 +296,14 @@ RingSchedule build_ring_schedule(const std::vector<MatrixTerm> &terms, uint32_t 
         uint32_t m_lo = 0, jh = 0;
         std::vector<PGroup> groups;
     };
+    auto pattern_of = [&](const Item &it) {
+        const uint32_t zj = static_cast<uint32_t>((it.z & inner) >> L);
+        uint32_t pattern = 0;
+        for (uint32_t j = 0; j < 8; ++j) pattern |= (static_cast<uint32_t>(__builtin_popcount(zj & j)) & 1u) << j;
+        return pattern;
+    };
+    // run of a record: real / imaginary weight x uniform / patterned sign
+    auto run_of = [&](const Item &it) { return (it.imag << 1) | (pattern_of(it) != 0u ? 1u : 0u); };
     std::vector<PCoset> pend;
     size_t pend_groups = 0, pend_terms = 0;
     uint64_t cur_d = 0;
@@ -318,13 +327,16 @@ RingSchedule build_ring_schedule(const std::vector<MatrixTerm> &terms, uint32_t 
         while ((r.blocks_c128.size() - off) % 16) r.blocks_c128.push_back(0);
         for (auto &c : pend) {
             for (auto &g : c.groups) {
+                // records of a group in four runs: real uniform-sign, real
+                // patterned, imaginary uniform-sign, imaginary patterned
+                std::stable_sort(g.items.begin(), g.items.end(),
+                                 [&](size_t u, size_t v) { return run_of(items[u]) < run_of(items[v]); });
                 for (size_t k : g.items) {
                     const Item &it = items[k];
                     const uint64_t zt = it.z >> S;
                     const uint32_t zlo = static_cast<uint32_t>(it.z & tmask);
                     const uint32_t zj = static_cast<uint32_t>((it.z & inner) >> L);
-                    uint32_t pattern = 0;
-                    for (uint32_t j = 0; j < 8; ++j) pattern |= (static_cast<uint32_t>(__builtin_popcount(zj & j)) & 1u) << j;
+                    const uint32_t pattern = pattern_of(it);
                     const bool flip = ((__builtin_popcountll(zt & cur_d) + __builtin_popcount(zlo & it.m_lo) +
                                         __builtin_popcount(zj & it.jh)) & 1) != 0;
                     const double w = flip ? -it.w : it.w;
