@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 //    waits (bounded) for the last fill of every stage before the block exits,
 //    so no copy is left writing into a finished block's memory.
 constexpr uint32_t kRingWarps = kThreads / 32;  // warps that own the tile's rows
-constexpr uint32_t kRingCompensateGroups = 8;  // FP32: groups per Kahan fold
+constexpr uint32_t kRingCompensateGroups = 16;  // FP32: groups per Kahan fold
 
 // Who refills the ring.  complex128: a dedicated producer warp waits on the
 // stages' "empty" barriers and issues the fills (measured faster for FP64,
@@ -272,7 +272,7 @@ template <> struct RingShape<float> {
 
 template <typename R> struct RingDepth;
 template <> struct RingDepth<double> { static constexpr uint32_t K = 3; };  // 3 x (64 + 8) KiB
-template <> struct RingDepth<float> { static constexpr uint32_t K = 5; };   // 5 x (32 + 8) KiB
+template <> struct RingDepth<float> { static constexpr uint32_t K = 4; };   // 4 x (32 + 8) KiB
 
 template <typename R> constexpr uint32_t ring_tile_bytes() {
     return (1u << kTileBitsC128) * static_cast<uint32_t>(sizeof(typename Cx<R>::T));
