@@ -18,7 +18,8 @@ from typing import Any, Optional, Tuple
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIBRARY_PATH = os.path.join(_HERE, "_lib", "libtcpmvp.so")
+# TCP_LIBRARY=debug loads the TCP_DEBUG_BOUNDS build (python -m tencirpauli_b200.build --debug-bounds)
+LIBRARY_PATH = os.path.join(_HERE, "_lib", "libtcpmvp_debug.so" if os.environ.get("TCP_LIBRARY") == "debug" else "libtcpmvp.so")
 
 # Status codes of include/tcp_mvp.h
 TCP_OK = 0

@@ -34,8 +34,17 @@ def _host_compiler() -> List[str]:
     return ["-ccbin", gxx] if os.path.exists(gxx) else []
 
 
-def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
+DEBUG_LIBPATH = os.path.join(LIBDIR, "libtcpmvp_debug.so")
+
+
+def build(verbose: bool = False, ptxas_verbose: bool = False, debug_bounds: bool = False) -> str:
+    """Compile the library.  ``debug_bounds`` builds ``libtcpmvp_debug.so``
+    with TCP_DEBUG_BOUNDS: the hot kernel checks every plan block against its
+    shared-memory stage before walking it and reports a failed check as
+    TCP_ERR_INVALID_ARGUMENT instead of reading outside the stage.  Select it
+    at run time with TCP_LIBRARY=debug."""
     os.makedirs(LIBDIR, exist_ok=True)
+    target = DEBUG_LIBPATH if debug_bounds else LIBPATH
     cmd = [
         nvcc(),
         *ARCH,
@@ -48,8 +57,10 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
         "-fPIC,-O3",
         "--expt-relaxed-constexpr",
         "-o",
-        LIBPATH + ".tmp",
+        target + ".tmp",
     ]
+    if debug_bounds:
+        cmd += ["-DTCP_DEBUG_BOUNDS"]
     if ptxas_verbose:
         cmd += ["-Xptxas", "-v"]
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
@@ -60,9 +71,10 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
         raise RuntimeError(f"nvcc failed:\n{proc.stdout}\n{proc.stderr}")
     if ptxas_verbose or verbose:
         sys.stdout.write(proc.stdout + proc.stderr)
-    os.replace(LIBPATH + ".tmp", LIBPATH)
-    _write_build_info()
-    return LIBPATH
+    os.replace(target + ".tmp", target)
+    if not debug_bounds:
+        _write_build_info()
+    return target
 
 
 def _git(*args: str) -> str:
@@ -94,4 +106,4 @@ def _write_build_info() -> None:
 
 
 if __name__ == "__main__":
-    build(verbose=True, ptxas_verbose="-v" in sys.argv)
+    build(verbose=True, ptxas_verbose="-v" in sys.argv, debug_bounds="--debug-bounds" in sys.argv)

@@ -545,6 +545,7 @@ extern "C" int tcp_mvp_batch_configure(tcp_mvp_batch *b, uint32_t tile_rows_log2
 }
 
 extern "C" int tcp_mvp_batch_apply(tcp_mvp_batch *b, const void *const *d_x, void *const *d_y, void *stream) {
+    tcp::Range range("tcp_mvp_batch_apply");
     int st = check_batch(b);
     if (st) return st;
     if (d_x == nullptr || d_y == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer table");

@@ -26,6 +26,7 @@ constexpr uint32_t kNoPasses = 0xffffffffu;
 
 // Error bits written by kernels into the plan's device status word.
 constexpr int kErrTimeout = 1;
+constexpr int kErrBounds = 2;  // TCP_DEBUG_BOUNDS builds: a block failed its bounds check
 
 struct DevSchedule {
     // step view (tiled kernels); see tcp::Schedule

@@ -10,7 +10,20 @@
 
 #include "../../include/tcp_mvp.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace tcp {
+
+// NVTX range over a scope (plan building, uploads, applies), so that a
+// timeline profiler shows where the host side of the library spends its
+// time.  NVTX is header-only and costs a null-function call when no tool is
+// attached.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
 
 // Thread-local last-error slot behind tcp_last_error().
 void set_error(const std::string &message);

@@ -344,6 +344,22 @@ __device__ __forceinline__ void ring_group(const uint4 *__restrict__ trm, uint32
     if (k < nt) ring_term<A, R>(trm[k], tid, tile32, xv, acc);
 }
 
+#ifdef TCP_DEBUG_BOUNDS
+// A block stays inside its `bytes`: header, coset records, group words and
+// the records they count; thread-bit masks below 512, permutations below 8.
+__device__ __forceinline__ bool ring_block_in_bounds(uint4 hdr, const uint4 *cos, const uint32_t *gw, uint32_t bytes) {
+    if (bytes > tcp::kRingBlockBytes || 16u + 16u * hdr.x + 4u * hdr.y > 16u * hdr.z || 16u * hdr.z > bytes) return false;
+    uint32_t groups = 0, records = 0;
+    for (uint32_t c = 0; c < hdr.x; ++c) {
+        if (cos[c].x >= 512u || cos[c].y >= 8u) return false;
+        groups += cos[c].z;
+    }
+    if (groups != hdr.y) return false;
+    for (uint32_t g = 0; g < groups; ++g) records += gw[g] >> 4;
+    return 16u * hdr.z + 16u * records <= bytes;
+}
+#endif
+
 // Issue the fill of ring step `i` (source tile and block) into its stage.
 template <typename R>
 __device__ __forceinline__ void ring_fill(const DevSchedule &s, const typename Cx<R>::T *__restrict__ x,
@@ -457,10 +473,18 @@ __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
         }
         const C *xs = reinterpret_cast<const C *>(smem_raw + stage * STAGE);
         const unsigned char *blk = smem_raw + stage * STAGE + TILE_BYTES;
-        const uint4 hdr = *reinterpret_cast<const uint4 *>(blk);
+        uint4 hdr = *reinterpret_cast<const uint4 *>(blk);
         const uint4 *cos = reinterpret_cast<const uint4 *>(blk + 16);
         const uint32_t *gw = reinterpret_cast<const uint32_t *>(blk + 16u + hdr.x * 16u);
         const uint4 *trm = reinterpret_cast<const uint4 *>(blk + hdr.z * 16u);
+#ifdef TCP_DEBUG_BOUNDS
+        // debug builds check every block against its stage before walking it
+        // and skip (recording kErrBounds) a block that would read outside it
+        if (!ring_block_in_bounds(hdr, cos, gw, __ldg(&info[st]).w * 16u)) {
+            if (lane == 0u) atomicOr(err, kErrBounds);
+            hdr.x = 0u;
+        }
+#endif
         uint32_t g = 0;
         for (uint32_t c = 0; c < hdr.x; ++c) {
             const uint4 cr = cos[c];
@@ -687,6 +711,7 @@ void set_passes(const std::vector<uint32_t> &step_info, uint32_t tile_bits, uint
 
 // Lay both schedules out in one device allocation.
 int upload(tcp_mvp_plan *p) {
+    tcp::Range range("plan upload");
     struct Piece {
         const void *src;
         size_t bytes;
@@ -866,6 +891,7 @@ int read_device_status(const tcp_mvp_plan *p) {
         int zero = 0;
         cudaMemcpy(p->d_err, &zero, sizeof(int), cudaMemcpyHostToDevice);
         if (h & kErrTimeout) return fail(TCP_ERR_DEVICE_TIMEOUT, "a bounded device-side wait expired");
+        if (h & kErrBounds) return fail(TCP_ERR_INVALID_ARGUMENT, "a plan block failed its bounds check (TCP_DEBUG_BOUNDS)");
     }
     return TCP_OK;
 }
@@ -962,6 +988,7 @@ struct HostCopies {
         return slot;
     }
     int to_device(void *dst, const void *src, size_t len, cudaStream_t s) {
+        tcp::Range range(stage_in ? "staged H2D" : "H2D");
         if (!stage_in) {
             cudaError_t e = cudaMemcpyAsync(dst, src, len, cudaMemcpyHostToDevice, s);
             return e == cudaSuccess ? TCP_OK : cuda_fail(e, "H2D copy");
@@ -987,6 +1014,7 @@ struct HostCopies {
         return TCP_OK;
     }
     int to_host(void *dst, const void *src, size_t len, cudaStream_t s) {
+        tcp::Range range(stage_out ? "staged D2H" : "D2H");
         if (!stage_out) {
             cudaError_t e = cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToHost, s);
             return e == cudaSuccess ? TCP_OK : cuda_fail(e, "D2H copy");
@@ -1051,6 +1079,7 @@ void release_staging(tcp::Staging *stage) {
 
 template <typename R>
 int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *result, uint64_t result_len) {
+    tcp::Range range(sizeof(R) == 8 ? "tcp_mvp_apply_into_host" : "tcp_mvp_apply_into_host_c64");
     int st = check_plan(plan);
     if (st) return st;
     if (state_len != plan->dim) return length_error(plan->dim, state_len);
@@ -1205,6 +1234,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
 extern "C" int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32_t word_count,
                                    const uint64_t *x_words, const uint64_t *z_words, const double *coefficients,
                                    int storage, uint64_t max_bytes, tcp_mvp_plan **out_plan) {
+    tcp::Range range("tcp_mvp_plan_create");
     if (out_plan == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "out_plan is null");
     *out_plan = nullptr;
     if (storage != TCP_STORAGE_LAZY && storage != TCP_STORAGE_EAGER) {
@@ -1246,8 +1276,11 @@ extern "C" int tcp_mvp_plan_create(uint32_t nqubits, uint64_t term_count, uint32
     cudaError_t e = cudaGetDevice(&p->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (g_num_sms == 0) cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, p->device);
-    p->sched.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
-    p->sched.ring = tcp::build_ring_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
+    {
+        tcp::Range range("tile schedules");
+        p->sched.host = tcp::build_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
+        p->sched.ring = tcp::build_ring_schedule(p->terms, nqubits, kTileBitsC128, kLogThreads);
+    }
     st = upload(p.get());
     if (st) return st;
     if (storage == TCP_STORAGE_EAGER) {
@@ -1313,6 +1346,7 @@ extern "C" int tcp_mvp_apply_into_host_c64(const tcp_mvp_plan *plan, const float
 namespace {
 int apply_device(const tcp_mvp_plan *plan, const void *d_state, void *d_result, uint64_t len, uint32_t nrhs,
                  int dtype, void *stream, bool accumulate) {
+    tcp::Range range(accumulate ? "tcp_mvp_apply_add_device" : "tcp_mvp_apply_into_device");
     int st = check_plan(plan);
     if (st) return st;
     if (len != plan->dim) return length_error(plan->dim, len);

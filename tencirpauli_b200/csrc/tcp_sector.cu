@@ -1683,6 +1683,7 @@ extern "C" int tcp_u1_plan_create(uint32_t nqubits, uint32_t particle_number, ui
                                   uint32_t word_count, const uint64_t *x_words, const uint64_t *z_words,
                                   const double *coefficients, int storage, uint64_t max_bytes,
                                   tcp_u1_plan **out_plan) {
+    tcp::Range range("tcp_u1_plan_create");
     if (out_plan == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "out_plan is null");
     *out_plan = nullptr;
     if (storage != TCP_STORAGE_LAZY && storage != TCP_STORAGE_EAGER) {
@@ -1789,6 +1790,7 @@ extern "C" int tcp_u1_plan_info(const tcp_u1_plan *plan, tcp_u1_plan_info_t *inf
 
 extern "C" int tcp_u1_apply_into_host(const tcp_u1_plan *plan, const double *state, uint64_t state_len,
                                       double *result, uint64_t result_len, uint64_t max_bytes) {
+    tcp::Range range("tcp_u1_apply_into_host");
     (void)max_bytes;  // advisory: the output is caller-owned
     return apply_host<double>(plan, state, state_len, result, result_len);
 }

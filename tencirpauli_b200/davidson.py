@@ -46,6 +46,45 @@ class DavidsonResult:
     preconditioner: str = ""
 
 
+CHECKPOINT_VERSION = 1
+
+
+def save_checkpoint(path: str, ritz: Any, phase: int, iterations: int, theta: Any) -> None:
+    """Write the lowest Ritz vectors of the current subspace (FP64 on the
+    host), the precision phase (0: complex64 MVP, 1: FP64) and the iteration
+    count to a versioned ``.npz``; ``davidson(start=path)`` resumes from it.
+    The file is written next to its final name and renamed, so an
+    interrupted write leaves the previous checkpoint intact."""
+    import torch
+
+    tmp = path + ".tmp.npz"
+    np.savez(
+        tmp,
+        version=np.int64(CHECKPOINT_VERSION),
+        ritz=ritz.to(torch.complex128).cpu().numpy(),
+        phase=np.int64(phase),
+        iterations=np.int64(iterations),
+        theta=np.asarray(theta.cpu().numpy() if hasattr(theta, "cpu") else theta, dtype=np.float64),
+    )
+    import os
+
+    os.replace(tmp, path)
+
+
+def load_checkpoint(path: str):
+    """(start block on the device, phase, iterations) from ``save_checkpoint``."""
+    import torch
+
+    with np.load(path) as data:
+        if int(data["version"]) != CHECKPOINT_VERSION:
+            raise ValueError(f"unsupported Davidson checkpoint version {int(data['version'])}")
+        ritz = data["ritz"]
+        phase = int(data["phase"])
+        iterations = int(data["iterations"])
+    dtype = torch.complex64 if phase == 0 else torch.complex128
+    return torch.from_numpy(ritz).to("cuda").to(dtype), phase, iterations
+
+
 class JacobiPreconditioner:
     """t = -r / (H_ii - theta): the plain diagonal (Davidson) correction."""
 
@@ -93,6 +132,8 @@ def davidson(
     start: Optional[Any] = None,
     record_history: bool = False,
     callback: Optional[Any] = None,
+    checkpoint: Optional[str] = None,
+    checkpoint_every: int = 25,
 ) -> DavidsonResult:
     import torch
 
@@ -112,18 +153,24 @@ def davidson(
     # and every later Gram / combine pass read fewer basis vectors.
     keep = keep or min(max_subspace - block, max(2 * (nev + block), max_subspace // 4))
 
-    if start is None:
+    resume_phase = 0
+    done_iterations = 0
+    if isinstance(start, str):
+        X, resume_phase, done_iterations = load_checkpoint(start)
+    elif start is None:
         X = random_state_device(execution.nqubits, seed=seed, dtype=torch.complex64, nrhs=block, length=n)
     else:
         X = start
-    iterations = 0
+    iterations = done_iterations if isinstance(start, str) else 0
     mvps = 0
     fallbacks = 0
     history: List[np.ndarray] = []
     phase_iterations: List[int] = []
     theta = None
     U = None
-    for dtype, phase_tol in ((torch.complex64, switch_tol), (torch.complex128, tol)):
+    for phase_index, (dtype, phase_tol) in enumerate(((torch.complex64, switch_tol), (torch.complex128, tol))):
+        if phase_index < resume_phase:
+            continue
         drop = 1e-10 if dtype == torch.complex128 else 1e-5
         V = torch.empty((max_subspace, n), dtype=dtype, device="cuda")
         W = torch.empty_like(V)
@@ -183,6 +230,11 @@ def davidson(
                     X = torch.empty((carry, n), dtype=dtype, device="cuda")
                     solver_ops.combine(V[:m], evecs[:, :carry], X)
                 break
+            if checkpoint is not None and iterations % checkpoint_every == 0:
+                Uc = torch.empty((keep if m >= keep else m, n), dtype=dtype, device="cuda")
+                solver_ops.combine(V[:m], evecs[:, : Uc.shape[0]], Uc)
+                save_checkpoint(checkpoint, Uc, phase_index, iterations, theta)
+                del Uc
             idx = [j for j in range(nev) if norms[j] > phase_tol][:block]
             Rsel = R[idx].contiguous()
             Tc = torch.empty_like(Rsel)

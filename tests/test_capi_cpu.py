@@ -214,3 +214,22 @@ def test_noalloc_entry_point_names_no_allocating_routine() -> None:
     forbidden = ("cudaMalloc", "cudaFree", "dev_malloc", "cudaHostAlloc", "cudaMallocHost", "malloc(", "new ")
     for name in forbidden:
         assert name not in body, f"{name} appears in the allocation-free path"
+
+
+def test_debug_bounds_build_compiles() -> None:
+    """The TCP_DEBUG_BOUNDS variant of the hot kernel's translation unit
+    compiles for sm_100a (the full library is built on demand with
+    ``python -m tencirpauli_b200.build --debug-bounds``)."""
+    import subprocess
+    import tempfile
+
+    from tencirpauli_b200 import build
+
+    src = os.path.join(ROOT, "tencirpauli_b200", "csrc", "tcp_mvp.cu")
+    with tempfile.TemporaryDirectory() as tmp:
+        proc = subprocess.run(
+            [build.nvcc(), *build.ARCH, "-O1", "-std=c++17", "--expt-relaxed-constexpr", "-DTCP_DEBUG_BOUNDS", "-c", src,
+             "-o", os.path.join(tmp, "tcp_mvp_debug.o")],
+            capture_output=True, text=True,
+        )
+    assert proc.returncode == 0, proc.stderr[-2000:]

@@ -174,6 +174,26 @@ def test_davidson_matches_dense_eigenvalues_with_exact_residuals() -> None:
     assert res.phase_iterations and len(res.phase_iterations) == 2
 
 
+def test_davidson_checkpoint_and_resume(tmp_path) -> None:
+    """A run stopped early leaves a checkpoint of its lowest Ritz vectors
+    (FP64, versioned .npz); a new run started from it converges to the dense
+    eigenvalues with exact residuals, and continues the iteration count."""
+    op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(3, 4, 1.0, 0.5))
+    plan = op.native_mvp_plan()
+    ref = np.linalg.eigvalsh(_dense(op))[:4]
+    path = str(tmp_path / "dav.npz")
+    first = davidson(plan, nev=4, tol=1e-8, seed=3, max_iter=14, checkpoint=path, checkpoint_every=5)
+    assert not first.converged
+    with np.load(path) as data:
+        assert int(data["version"]) == 1 and int(data["iterations"]) == 10
+        assert data["ritz"].dtype == np.complex128 and data["ritz"].shape[1] == plan.dimension
+    resumed = davidson(plan, nev=4, tol=1e-8, start=path)
+    assert resumed.converged
+    np.testing.assert_allclose(resumed.eigenvalues, ref, rtol=0, atol=1e-9)
+    assert (resumed.residuals <= 1e-8).all()
+    assert resumed.iterations > 10
+
+
 def test_learned_preconditioner_runs_and_untrained_equals_jacobi() -> None:
     op = PauliOperator.from_code_arrays(*workloads.j1j2_periodic(4, 4, 1.0, 0.3))
     plan = op.native_mvp_plan()
