@@ -555,7 +555,11 @@ def run_chemistry(args: argparse.Namespace) -> None:
         res[name] = {"ms": ms, "amp_terms_per_s": op.term_count * (1 << n) / (ms / 1e3),
                      "rel_err_rows": float(np.linalg.norm(got - ref) / np.linalg.norm(ref))}
         del x, y
-    nrhs = 16
+    nrhs = args.chem_block_rhs
+    if nrhs <= 0:
+        print(json.dumps({"workload": f"Jordan-Wigner chemistry-like Hamiltonian, n={n}", "terms": op.term_count,
+                          "groups": plan.group_count, "host_build_s": build_s, "results": res}), flush=True)
+        return
     xs = [workloads.random_state_device(n, seed=args.seed + 1, dtype=torch.complex64, nrhs=nrhs)]
     ys = [torch.empty_like(xs[0])]
     batch = BatchedMVP([plan], nrhs=nrhs, dtype="complex64")
@@ -868,6 +872,8 @@ def main() -> None:
     parser.add_argument("--batch-count", type=int, default=64)
     parser.add_argument("--lattice", default="4x7", help="sector workload: periodic J1-J2 lattice LXxLY")
     parser.add_argument("--batch-rhs", type=int, default=8)
+    parser.add_argument("--chem-block-rhs", type=int, default=16,
+                        help="chemistry workload: right-hand sides of the batched complex64 block (0: skip it)")
     parser.add_argument("--batch-nmax", type=int, default=26, help="batched workload: largest member size")
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=10)
