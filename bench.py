@@ -353,8 +353,14 @@ def run_batched(args: argparse.Namespace) -> None:
     xs = [workloads.random_state_device(op.nqubits, seed=args.seed + i, dtype=dtype, nrhs=nrhs) for i, op in enumerate(ops)]
     ys = [torch.empty_like(x) for x in xs]
     batch = BatchedMVP(plans, nrhs=nrhs, dtype="complex64")
-    cache = os.path.join(tempfile.gettempdir(), "tcp_batch_autotune.txt")
-    tune = batch.autotune(xs, ys, cache_path=cache, repeats=2)
+    if args.batch_config:
+        logt, rb = (int(v) for v in args.batch_config.split(","))
+        batch.configure(logt, rb)
+        tune = dict(batch.info(), fixed=True)
+    else:
+        cache = os.path.join(tempfile.gettempdir(), "tcp_batch_autotune.txt")
+        tune = batch.autotune(xs, ys, cache_path=cache, repeats=2)
+    ring = tune["tile_rows_log2"] == 12
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         batch.apply(xs, ys, stream)
@@ -378,8 +384,9 @@ def run_batched(args: argparse.Namespace) -> None:
     state_bytes = sum((1 << op.nqubits) * nrhs * 8 for op in ops)
     peaks = _measured_peaks()
     achieved = 2 * state_bytes / (ms / 1000.0) / 1e9
-    # k_batched reads one 8-byte complex64 operand per (row, x-mask group,
-    # right-hand side) from shared memory: its binding ceiling is the
+    # Both batched kernels read one 8-byte complex64 operand per (row, x-mask
+    # group, right-hand side) from shared memory (the ring kernel once per
+    # coset of groups, so slightly less): the binding ceiling is the
     # shared-memory rate, probed on this GPU.
     from tencirpauli_b200 import _native as native_mod
 
@@ -428,7 +435,7 @@ def run_batched(args: argparse.Namespace) -> None:
             "frac": smem_ach / smem_rate,
             "traffic": None,
             "peak_source": "tcp_probe_smem_rate on this GPU, best of 5",
-            "kernel": "k_batched",
+            "kernel": "k_ring (one launch per member, blockIdx.y = RHS)" if ring else "k_batched",
             "smem_bytes_per_launch": smem_bytes,
             "fp": {"achieved": flops / (ms / 1000.0) / 1e12, "peak": fma_rate / 1e12, "unit": "TFLOP/s",
                    "frac": flops / (ms / 1000.0) / fma_rate},
@@ -436,7 +443,7 @@ def run_batched(args: argparse.Namespace) -> None:
                     "peak_source": peaks["source"]},
         },
         "e2e": None,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (tune["grid"] if ring else 1),
         "clocks": clocks,
         "accuracy": {"rel_err_vs_oracle_rows": errs},
     }
@@ -875,6 +882,9 @@ def main() -> None:
     parser.add_argument("--chem-block-rhs", type=int, default=16,
                         help="chemistry workload: right-hand sides of the batched complex64 block (0: skip it)")
     parser.add_argument("--batch-nmax", type=int, default=26, help="batched workload: largest member size")
+    parser.add_argument("--batch-config", default=None,
+                        help="batched workload: fixed 'tile_rows_log2,rhs_block' instead of the autotuner "
+                             "(12,1 = one ring-kernel launch per member)")
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=10)
     parser.add_argument("--warmup", type=int, default=3)

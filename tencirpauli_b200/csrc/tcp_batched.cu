@@ -13,11 +13,18 @@
 // current item's last step.  Per term, the sign and weight are evaluated once
 // and applied to all RB right-hand sides.
 //
+// The ring configuration (tile_rows_log2 = 12, rhs_block = 1) instead runs
+// the single-operator ring kernel once per member, its grid covering every
+// output tile and every right-hand side (blockIdx.y), members largest first,
+// all captured in the same CUDA graph.  It needs a ring schedule for every
+// member (n >= 12).
+//
 // State layout: the RHS block of Hamiltonian h is RHS-major, vector v at
 // offset v * 2^n (complex128 or complex64), as for tcp_mvp_apply_into_device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -192,9 +199,13 @@ struct Variant {
     uint32_t logt;
     uint32_t rb;
     bool c64;
-    const void *fn;
+    const void *fn;  // null for the ring configuration
     size_t smem;
 };
+
+constexpr uint32_t kRingLogt = 12;  // the ring configuration: (12, 1)
+
+Variant ring_variant(bool c64) { return Variant{kRingLogt, 1, c64, nullptr, 0}; }
 
 template <int LOGT, int RB, typename R> Variant make_variant() {
     Variant v;
@@ -215,7 +226,7 @@ const std::vector<Variant> &variants() {
         make_variant<8, 2, double>(), make_variant<8, 4, double>(), make_variant<8, 8, double>(),
         make_variant<9, 1, double>(), make_variant<9, 2, double>(), make_variant<9, 4, double>(),
         make_variant<9, 8, double>(), make_variant<10, 1, double>(), make_variant<10, 2, double>(),
-        make_variant<10, 4, double>(),
+        make_variant<10, 4, double>(), ring_variant(true), ring_variant(false),
     };
     return all;
 }
@@ -256,6 +267,8 @@ struct tcp_mvp_batch {
     unsigned int *d_counter = nullptr;
     int *d_err = nullptr;
     int grid = 0;
+    bool ring = false;                 // ring configuration: one launch per member
+    std::vector<uint32_t> ring_order;  // members with terms, largest first
     // graph
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -277,8 +290,44 @@ void release_config(tcp_mvp_batch *b) {
     b->d_items = nullptr;
     b->schedules.clear();
     b->hams_host.clear();
+    b->ring = false;
+    b->ring_order.clear();
     b->bound_x.clear();
     b->bound_y.clear();
+}
+
+// The ring configuration: no batch schedules or work list; every member's own
+// ring schedule serves its launch.
+int configure_ring(tcp_mvp_batch *b) {
+    if (b->nrhs > 65535u) return fail(TCP_ERR_INVALID_ARGUMENT, "the ring configuration takes at most 65535 right-hand sides");
+    for (const tcp_mvp_plan *p : b->plans) {
+        int st = tcp::ring_prepare(p, b->c64);
+        if (st) return st;
+    }
+    release_config(b);
+    b->logt = kRingLogt;
+    b->rb = 1;
+    b->ring = true;
+    b->hams_host.assign(b->plans.size(), BatchHam{});
+    b->empty_members.clear();
+    std::vector<std::pair<double, uint32_t>> order;
+    uint64_t ctas = 0;
+    for (size_t h = 0; h < b->plans.size(); ++h) {
+        const tcp_mvp_plan *p = b->plans[h];
+        b->hams_host[h].dim = p->dim;
+        b->hams_host[h].nqubits = p->nqubits;
+        if (p->sched.dev.ring_steps == 0) {
+            b->empty_members.push_back(static_cast<uint32_t>(h));
+            continue;
+        }
+        order.push_back({static_cast<double>(p->terms.size()) * static_cast<double>(p->dim), static_cast<uint32_t>(h)});
+        ctas += (p->dim >> kRingLogt) * b->nrhs;
+    }
+    std::stable_sort(order.begin(), order.end(), [](const auto &a, const auto &c) { return a.first > c.first; });
+    for (const auto &o : order) b->ring_order.push_back(o.second);
+    b->nitems = static_cast<uint32_t>(std::min<uint64_t>(ctas, 0xffffffffull));
+    b->grid = static_cast<int>(b->ring_order.size());
+    return TCP_OK;
 }
 
 // Build schedules, the work list and the device tables for (logt, rb).
@@ -286,6 +335,7 @@ int configure(tcp_mvp_batch *b, uint32_t logt, uint32_t rb) {
     const Variant *v = find_variant(logt, rb, b->c64);
     if (v == nullptr) return fail(TCP_ERR_INVALID_ARGUMENT, "no batched kernel variant for this tile / RHS block");
     if (b->nrhs % rb != 0) return fail(TCP_ERR_INVALID_ARGUMENT, "the RHS block must divide the RHS count");
+    if (v->fn == nullptr) return configure_ring(b);
     for (const tcp_mvp_plan *p : b->plans) {
         if (p->nqubits < logt) {
             return fail(TCP_ERR_INVALID_ARGUMENT, "every batch member needs at least " + std::to_string(logt) +
@@ -394,7 +444,7 @@ int bind_buffers(tcp_mvp_batch *b, const void *const *d_x, void *const *d_y, cud
         b->hams_host[h].x = d_x[h];
         b->hams_host[h].y = d_y[h];
     }
-    if (*changed && !b->hams_host.empty()) {
+    if (*changed && !b->hams_host.empty() && !b->ring) {
         cudaError_t e = cudaMemcpyAsync(b->d_hams, b->hams_host.data(), sizeof(BatchHam) * b->hams_host.size(),
                                         cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) return cuda_fail(e, "batch descriptor upload");
@@ -404,6 +454,17 @@ int bind_buffers(tcp_mvp_batch *b, const void *const *d_x, void *const *d_y, cud
 
 // Record the batch's launch sequence on `s` (used under stream capture).
 int record_launch(tcp_mvp_batch *b, cudaStream_t s) {
+    if (b->ring) {
+        for (uint32_t h : b->empty_members) {
+            cudaError_t e = cudaMemsetAsync(b->hams_host[h].y, 0, b->plans[h]->dim * b->nrhs * (b->c64 ? 8 : 16), s);
+            if (e != cudaSuccess) return cuda_fail(e, "zeroing an empty member");
+        }
+        for (uint32_t h : b->ring_order) {
+            int st = tcp::launch_ring_rhs(b->plans[h], b->hams_host[h].x, b->hams_host[h].y, b->nrhs, b->c64, b->d_err, s);
+            if (st) return st;
+        }
+        return TCP_OK;
+    }
     const Variant *v = find_variant(b->logt, b->rb, b->c64);
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned int), s);
     if (e != cudaSuccess) return cuda_fail(e, "batch counter reset");
@@ -443,9 +504,11 @@ int apply_locked(tcp_mvp_batch *b, const void *const *d_x, void *const *d_y, cud
     bool changed = false;
     int st = bind_buffers(b, d_x, d_y, stream, &changed);
     if (st) return st;
-    // The graph only captures pointers to device tables, except the memsets of
-    // empty members' outputs; rebuild it when the configuration or those change.
-    if (b->graph == nullptr || (changed && !b->empty_members.empty())) {
+    // The persistent kernel's graph only captures pointers to device tables,
+    // except the memsets of empty members' outputs; the ring configuration's
+    // launches take the buffers themselves.  Rebuild the graph when the
+    // configuration or the captured buffers change.
+    if (b->graph == nullptr || (changed && (b->ring || !b->empty_members.empty()))) {
         st = build_graph(b);
         if (st) return st;
     }

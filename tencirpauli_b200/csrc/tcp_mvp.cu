@@ -35,6 +35,7 @@ using tcp::fail;
 
 #include "tcp_device.cuh"
 #include "tcp_plan_impl.h"
+#include "tcp_ring.cuh"
 
 using namespace tcpdev;
 
@@ -251,99 +252,6 @@ __global__ void __launch_bounds__(kThreads, 1)
 //    CTA's abort word; the kernel then records kErrTimeout, and thread 0
 //    waits (bounded) for the last fill of every stage before the block exits,
 //    so no copy is left writing into a finished block's memory.
-constexpr uint32_t kRingWarps = kThreads / 32;  // warps that own the tile's rows
-constexpr uint32_t kRingCompensateGroups = 16;  // FP32: groups per Kahan fold
-
-// Who refills the ring.  complex128: a dedicated producer warp waits on the
-// stages' "empty" barriers and issues the fills (measured faster for FP64,
-// whose row warps fit the 96 registers a 544-thread block leaves them).
-// complex64: no extra warp -- the row warp that releases a stage last issues
-// its refill -- so the 512 threads keep 128 registers for the paired FP32
-// accumulators.
-template <typename R> struct RingShape;
-template <> struct RingShape<double> {
-    static constexpr bool kProducerWarp = true;
-    static constexpr int kThreadsPerCta = kThreads + 32;
-};
-template <> struct RingShape<float> {
-    static constexpr bool kProducerWarp = false;
-    static constexpr int kThreadsPerCta = kThreads;
-};
-
-template <typename R> struct RingDepth;
-template <> struct RingDepth<double> { static constexpr uint32_t K = 3; };  // 3 x (64 + 8) KiB
-template <> struct RingDepth<float> { static constexpr uint32_t K = 4; };   // 4 x (32 + 8) KiB
-
-template <typename R> constexpr uint32_t ring_tile_bytes() {
-    return (1u << kTileBitsC128) * static_cast<uint32_t>(sizeof(typename Cx<R>::T));
-}
-template <typename R> constexpr uint32_t ring_stage_bytes() { return ring_tile_bytes<R>() + tcp::kRingBlockBytes; }
-template <typename R> constexpr size_t ring_smem_bytes() {
-    return static_cast<size_t>(RingDepth<R>::K) * ring_stage_bytes<R>();
-}
-
-template <typename R> __device__ __forceinline__ const unsigned char *ring_blocks(const DevSchedule &s);
-template <> __device__ __forceinline__ const unsigned char *ring_blocks<double>(const DevSchedule &s) {
-    return s.ring128;
-}
-template <> __device__ __forceinline__ const unsigned char *ring_blocks<float>(const DevSchedule &s) {
-    return s.ring64;
-}
-
-// Weight of a ring term record: one f64 (bytes 8..15) or one f32 (bytes 8..11).
-template <typename R> __device__ __forceinline__ R ring_weight(uint4 rec);
-template <> __device__ __forceinline__ double ring_weight<double>(uint4 rec) {
-    return __hiloint2double(static_cast<int>(rec.w), static_cast<int>(rec.z));
-}
-template <> __device__ __forceinline__ float ring_weight<float>(uint4 rec) { return __uint_as_float(rec.z); }
-
-// One term record applied to the thread's 8 rows, row j reading loaded value
-// j ^ A.  Sign of row j: parity(zlo & t) ^ parity(zt & tile) ^ bit j of the
-// pattern (the rest is folded into the weight).  meta & t keeps only the zlo
-// bits because t < 512.
-template <int A, typename R>
-__device__ __forceinline__ void ring_term(uint4 rec, uint32_t tid, uint32_t tile32,
-                                          const typename Cx<R>::T (&xv)[8], RingAcc<R> (&acc)[8]) {
-    const uint32_t meta = rec.x;
-    const uint32_t base = __popc((meta & tid) ^ (rec.y & tile32)) & 1u;
-    const uint32_t pattern = (meta >> 9) & 0xffu;
-    const bool imag = ((meta >> 17) & 1u) != 0u;
-    const R w = ring_weight<R>(rec);
-    if (pattern == 0u) {
-        const R ws = flip_by(w, base);
-        if (!imag) {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j].add_real(ws, xv[j ^ A]);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j].add_imag(ws, xv[j ^ A]);
-        }
-    } else {
-        const uint32_t pat = (pattern ^ (0u - base)) & 0xffu;
-        if (!imag) {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j].add_real(flip_if(w, pat, j), xv[j ^ A]);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j].add_imag(flip_if(w, pat, j), xv[j ^ A]);
-        }
-    }
-}
-
-// The `nt` records of one group, two per iteration so that the integer work of
-// one overlaps the multiply-adds of the other.
-template <int A, typename R>
-__device__ __forceinline__ void ring_group(const uint4 *__restrict__ trm, uint32_t nt, uint32_t tid, uint32_t tile32,
-                                           const typename Cx<R>::T (&xv)[8], RingAcc<R> (&acc)[8]) {
-    uint32_t k = 0;
-    for (; k + 2u <= nt; k += 2u) {
-        const uint4 r0 = trm[k], r1 = trm[k + 1];
-        ring_term<A, R>(r0, tid, tile32, xv, acc);
-        ring_term<A, R>(r1, tid, tile32, xv, acc);
-    }
-    if (k < nt) ring_term<A, R>(trm[k], tid, tile32, xv, acc);
-}
-
 #ifdef TCP_DEBUG_BOUNDS
 // A block stays inside its `bytes`: header, coset records, group words and
 // the records they count; thread-bit masks below 512, permutations below 8.
@@ -381,7 +289,7 @@ __device__ __forceinline__ void ring_fill(const DevSchedule &s, const typename C
 template <typename R, bool PASSES>
 __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
     k_ring(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
-           int *__restrict__ err, uint64_t tile0, uint32_t pass, uint32_t accumulate) {
+           int *__restrict__ err, uint64_t tile0, uint32_t pass, uint32_t accumulate, uint64_t rhs_stride) {
     using C = typename Cx<R>::T;
     constexpr uint32_t K = RingDepth<R>::K;
     constexpr uint32_t TILE_BYTES = ring_tile_bytes<R>();
@@ -397,6 +305,9 @@ __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint64_t tile = tile0 + blockIdx.x;
+    // blockIdx.y selects the right-hand side of an RHS-major block
+    x += blockIdx.y * rhs_stride;
+    y += blockIdx.y * rhs_stride;
     uint32_t step0 = 0, nsteps = s.ring_steps;
     if constexpr (PASSES) {
         const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.ring_pass_shift)) & (kPassChunks - 1u);
@@ -854,10 +765,10 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
         if (pass >= 0) {
             k_ring<R, true><<<static_cast<unsigned>(tiles), RingShape<R>::kThreadsPerCta, smem, stream>>>(
                 ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, static_cast<uint32_t>(pass),
-                accumulate ? 1u : 0u);
+                accumulate ? 1u : 0u, 0ull);
         } else {
             k_ring<R, false><<<static_cast<unsigned>(tiles), RingShape<R>::kThreadsPerCta, smem, stream>>>(
-                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, accumulate ? 1u : 0u);
+                ds.dev, static_cast<const C *>(x), static_cast<C *>(y), p->d_err, tile0, 0u, accumulate ? 1u : 0u, 0ull);
         }
     } else if (p->nqubits >= S && ds.host.tile_bits == S && aligned) {
         int st = ensure_smem_attrs<R>(p->device);
@@ -882,6 +793,46 @@ int launch_one(const tcp_mvp_plan *p, const void *x, void *y, cudaStream_t strea
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "MVP kernel launch");
 }
+
+}  // namespace
+
+namespace tcp {
+// Whether `p` can run the ring kernel, with its shared-memory opt-in for the
+// dtype set up (outside any stream capture).
+int ring_prepare(const tcp_mvp_plan *p, bool c64) {
+    if (p->sched.ring.tile_bits != kTileBitsC128 || p->nqubits < kTileBitsC128)
+        return fail(TCP_ERR_INVALID_ARGUMENT, "the ring configuration needs a ring schedule (at least " +
+                                                  std::to_string(kTileBitsC128) + " qubits) for every batch member");
+    return c64 ? ensure_smem_attrs<float>(p->device) : ensure_smem_attrs<double>(p->device);
+}
+
+// One ring-kernel launch over every output tile of `p` and `nrhs`
+// right-hand sides stored RHS-major (vector v at offset v * dim); a timed-out
+// wait is recorded in `err`.  Fails with TCP_ERR_INVALID_ARGUMENT when the
+// plan has no ring schedule or the buffers are not 16-byte aligned.
+int launch_ring_rhs(const tcp_mvp_plan *p, const void *x, void *y, uint32_t nrhs, bool c64, int *err,
+                    cudaStream_t stream) {
+    if (!ring_ok(p, x) || (reinterpret_cast<uintptr_t>(y) % 16) != 0)
+        return fail(TCP_ERR_INVALID_ARGUMENT, "the ring kernel needs a ring schedule and 16-byte aligned buffers");
+    if (nrhs == 0 || nrhs > 65535u) return fail(TCP_ERR_INVALID_ARGUMENT, "RHS count out of range for one launch");
+    const dim3 grid(static_cast<unsigned>(p->dim >> kTileBitsC128), nrhs);
+    if (c64) {
+        int st = ensure_smem_attrs<float>(p->device);
+        if (st != TCP_OK) return st;
+        k_ring<float, false><<<grid, RingShape<float>::kThreadsPerCta, ring_smem_bytes<float>(), stream>>>(
+            p->sched.dev, static_cast<const float2 *>(x), static_cast<float2 *>(y), err, 0ull, 0u, 0u, p->dim);
+    } else {
+        int st = ensure_smem_attrs<double>(p->device);
+        if (st != TCP_OK) return st;
+        k_ring<double, false><<<grid, RingShape<double>::kThreadsPerCta, ring_smem_bytes<double>(), stream>>>(
+            p->sched.dev, static_cast<const double2 *>(x), static_cast<double2 *>(y), err, 0ull, 0u, 0u, p->dim);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "ring kernel launch");
+}
+}  // namespace tcp
+
+namespace {
 
 int read_device_status(const tcp_mvp_plan *p) {
     int h = 0;
@@ -1542,7 +1493,7 @@ extern "C" int tcp_mvp_apply_into_host_noalloc(const tcp_mvp_plan *plan, const d
     const uint32_t S = kTileBitsC128;
     if (ring_ok(plan, dx)) {
         k_ring<double, false><<<static_cast<unsigned>(plan->dim >> S), RingShape<double>::kThreadsPerCta, ring_smem_bytes<double>(), s>>>(
-            ds.dev, dx, dy, d_status, 0, 0u, 0u);
+            ds.dev, dx, dy, d_status, 0, 0u, 0u, 0ull);
     } else if (plan->nqubits >= S && ds.host.tile_bits == S) {
         const size_t smem = tiled_smem_bytes<kLogRowsC128, double>();
         k_tiled<kLogRowsC128, double, false><<<static_cast<unsigned>(plan->dim >> S), kThreads, smem, s>>>(

@@ -63,4 +63,7 @@ namespace tcp {
 int check_plan(const tcp_mvp_plan *plan);
 int length_error(uint64_t expected, uint64_t actual);
 bool overlaps(const void *a, const void *b, size_t bytes);
+int ring_prepare(const tcp_mvp_plan *p, bool c64);
+int launch_ring_rhs(const tcp_mvp_plan *p, const void *x, void *y, uint32_t nrhs, bool c64, int *err,
+                    cudaStream_t stream);
 }  // namespace tcp

@@ -93,6 +93,53 @@ def test_every_variant_gives_the_same_result_and_graph_replays() -> None:
     batch.device_status()
 
 
+@pytest.mark.parametrize("dtype", ["complex128", "complex64"])
+def test_ring_configuration_matches_the_persistent_kernel(dtype: str) -> None:
+    # (12, 1): one ring-kernel launch per member over all tiles and RHS
+    ops = _members()[1:6] + [PauliOperator.empty(12)]
+    plans = [op.native_mvp_plan() for op in ops]
+    tdt = torch.complex128 if dtype == "complex128" else torch.complex64
+    nrhs = 3
+    xs, ys = _blocks(ops, nrhs, tdt)
+    batch = BatchedMVP(plans, nrhs=nrhs, dtype=dtype)
+    batch.configure(9, 1)
+    batch.apply(xs, ys)
+    torch.cuda.synchronize()
+    ref = [y.clone() for y in ys]
+    batch.configure(12, 1)
+    info = batch.info()
+    assert info["tile_rows_log2"] == 12 and info["rhs_block"] == 1 and info["grid"] == len(ops) - 1
+    for y in ys:
+        y.fill_(float("nan"))
+    batch.apply(xs, ys)
+    batch.apply(xs, ys)  # graph replay
+    torch.cuda.synchronize()
+    batch.device_status()
+    tol = 1e-13 if dtype == "complex128" else C64_NORM_RTOL
+    for op, x, y, r in zip(ops, xs, ys, ref):
+        if op.term_count == 0:
+            assert not torch.any(y != 0)
+            continue
+        rel = torch.linalg.vector_norm(y - r) / torch.linalg.vector_norm(r)
+        assert float(rel) <= tol, (op.nqubits, float(rel))
+    # new buffers: the captured launches are rebuilt around them
+    xs2, ys2 = _blocks(ops, nrhs, tdt)
+    batch.apply(xs2, ys2)
+    torch.cuda.synchronize()
+    for op, x, y in zip(ops, xs2, ys2):
+        if op.term_count == 0:
+            continue
+        for v in range(nrhs):
+            want = _oracle_apply(op, x[v].cpu().numpy().astype(np.complex128))
+            got = y[v].cpu().numpy().astype(np.complex128)
+            err = np.linalg.norm(got - want) / np.linalg.norm(want)
+            assert err <= (FP64_RTOL if dtype == "complex128" else C64_NORM_RTOL), (op.nqubits, v, err)
+    # a member below 12 qubits has no ring schedule
+    small = BatchedMVP([op.native_mvp_plan() for op in _members()[:2]], nrhs=1, dtype=dtype)
+    with pytest.raises(ValueError, match="ring schedule"):
+        small.configure(12, 1)
+
+
 def test_autotune_picks_a_variant_and_caches_it(tmp_path) -> None:
     ops = _members()[1:5]
     plans = [op.native_mvp_plan() for op in ops]
@@ -100,7 +147,7 @@ def test_autotune_picks_a_variant_and_caches_it(tmp_path) -> None:
     batch = BatchedMVP(plans, nrhs=8, dtype="complex64")
     cache = tmp_path / "autotune.txt"
     info = batch.autotune(xs, ys, cache_path=str(cache), repeats=2)
-    assert info["tile_rows_log2"] in (8, 9, 10) and 8 % info["rhs_block"] == 0
+    assert info["tile_rows_log2"] in (8, 9, 10, 12) and 8 % info["rhs_block"] == 0
     text = cache.read_text().split()
     assert len(text) == 3 and int(text[1]) == info["tile_rows_log2"] and int(text[2]) == info["rhs_block"]
     again = BatchedMVP(plans, nrhs=8, dtype="complex64").autotune(xs, ys, cache_path=str(cache))
