@@ -286,7 +286,7 @@ __device__ __forceinline__ void ring_fill(const DevSchedule &s, const typename C
     bulk_copy_g2s(dst + TILE_BYTES, ring_blocks<R>(s) + static_cast<size_t>(in.z) * 16u, blk_bytes, &full[st]);
 }
 
-template <typename R, bool PASSES>
+template <typename R, bool PASSES, bool RHS_BLOCK = false>
 __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
     k_ring(DevSchedule s, const typename Cx<R>::T *__restrict__ x, typename Cx<R>::T *__restrict__ y,
            int *__restrict__ err, uint64_t tile0, uint32_t pass, uint32_t accumulate, uint64_t rhs_stride) {
@@ -305,9 +305,13 @@ __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
     const uint64_t tile = tile0 + blockIdx.x;
-    // blockIdx.y selects the right-hand side of an RHS-major block
-    x += blockIdx.y * rhs_stride;
-    y += blockIdx.y * rhs_stride;
+    if constexpr (RHS_BLOCK) {
+        // blockIdx.y selects the right-hand side of an RHS-major block (a
+        // separate instantiation, so the single-vector kernel keeps its
+        // registers)
+        x += blockIdx.y * rhs_stride;
+        y += blockIdx.y * rhs_stride;
+    }
     uint32_t step0 = 0, nsteps = s.ring_steps;
     if constexpr (PASSES) {
         const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.ring_pass_shift)) & (kPassChunks - 1u);
@@ -702,6 +706,9 @@ template <typename R> int set_ring_smem_attr() {
                                          static_cast<int>(bytes));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_ring<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ring<R, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(bytes));
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "cudaFuncSetAttribute");
 }
 
@@ -819,12 +826,12 @@ int launch_ring_rhs(const tcp_mvp_plan *p, const void *x, void *y, uint32_t nrhs
     if (c64) {
         int st = ensure_smem_attrs<float>(p->device);
         if (st != TCP_OK) return st;
-        k_ring<float, false><<<grid, RingShape<float>::kThreadsPerCta, ring_smem_bytes<float>(), stream>>>(
+        k_ring<float, false, true><<<grid, RingShape<float>::kThreadsPerCta, ring_smem_bytes<float>(), stream>>>(
             p->sched.dev, static_cast<const float2 *>(x), static_cast<float2 *>(y), err, 0ull, 0u, 0u, p->dim);
     } else {
         int st = ensure_smem_attrs<double>(p->device);
         if (st != TCP_OK) return st;
-        k_ring<double, false><<<grid, RingShape<double>::kThreadsPerCta, ring_smem_bytes<double>(), stream>>>(
+        k_ring<double, false, true><<<grid, RingShape<double>::kThreadsPerCta, ring_smem_bytes<double>(), stream>>>(
             p->sched.dev, static_cast<const double2 *>(x), static_cast<double2 *>(y), err, 0ull, 0u, 0u, p->dim);
     }
     cudaError_t e = cudaGetLastError();
