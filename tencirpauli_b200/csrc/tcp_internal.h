@@ -92,11 +92,12 @@ struct Schedule {
 // kRingBlockBytes), but the groups of a step are arranged in cosets: groups
 // whose inner masks agree on the thread bits (m & (2^log_threads - 1)) read
 // the same 2^(S - log_threads) source values per thread, in a permuted order,
-// so the values are loaded once per coset and every group of the coset
-// applies them through a compile-time register permutation a = jh ^ jh_load.
+// so the values are loaded once per coset, in row order (fixed offsets), and
+// every group of the coset applies them through a compile-time register
+// permutation a = jh (its inner-mask bits above the thread bits).
 // Block layout (16-byte units):
 //   header    {ncosets, ngroups, terms offset / 16, 0}
-//   cosets    {m_lo, jh_load, groups in the coset, 0} each
+//   cosets    {m_lo, 0, groups in the coset, 0} each
 //   groups    u32 each: a | nterms << 4, padded to 16 bytes; a group's
 //             records come in four runs (real weights with one sign for all
 //             rows of a thread, real with a row pattern, then the same for

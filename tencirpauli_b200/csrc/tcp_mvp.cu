@@ -259,7 +259,7 @@ __device__ __forceinline__ bool ring_block_in_bounds(uint4 hdr, const uint4 *cos
     if (bytes > tcp::kRingBlockBytes || 16u + 16u * hdr.x + 4u * hdr.y > 16u * hdr.z || 16u * hdr.z > bytes) return false;
     uint32_t groups = 0, records = 0;
     for (uint32_t c = 0; c < hdr.x; ++c) {
-        if (cos[c].x >= 512u || cos[c].y >= 8u) return false;
+        if (cos[c].x >= 512u || cos[c].y != 0u) return false;
         groups += cos[c].z;
     }
     if (groups != hdr.y) return false;
@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
             C xv[8];
             const C *src = xs + (tid ^ cr.x);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) xv[j] = src[(static_cast<uint32_t>(j) ^ cr.y) << kLogThreads];
+            for (int j = 0; j < 8; ++j) xv[j] = src[static_cast<uint32_t>(j) << kLogThreads];
             for (uint32_t k = 0; k < cr.z; ++k, ++g) {
                 const uint32_t word = gw[g];
                 const uint32_t nt = word >> 4;

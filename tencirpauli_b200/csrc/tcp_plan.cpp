@@ -373,12 +373,12 @@ RingSchedule build_ring_schedule(const std::vector<MatrixTerm> &terms, uint32_t 
         if (new_coset) {
             PCoset c;
             c.m_lo = it.m_lo;
-            c.jh = it.jh;
+            c.jh = 0;  // row-order loads: the permutation lives in each group's a
             pend.push_back(c);
         }
         if (new_group) {
             PGroup g;
-            g.a = it.jh ^ pend.back().jh;
+            g.a = it.jh;
             pend.back().groups.push_back(g);
             ++pend_groups;
         }
