@@ -570,7 +570,7 @@ extern "C" int tcp_mvp_batch_create(uint32_t count, const tcp_mvp_plan *const *p
         cudaFree(b->d_counter);
         return cuda_fail(e, "cudaStreamCreate");
     }
-    // default configuration: 512-row tiles, the largest RHS block dividing nrhs
+    // persistent-kernel default: 512-row tiles, the largest RHS block dividing nrhs
     uint32_t rb = 8;
     while (rb > 1 && nrhs % rb != 0) rb >>= 1;
     uint32_t logt = 9;
@@ -580,7 +580,12 @@ extern "C" int tcp_mvp_batch_create(uint32_t count, const tcp_mvp_plan *const *p
         cudaFree(b->d_counter);
         return fail(TCP_ERR_INVALID_ARGUMENT, "batched plans need at least 8 qubits");
     }
-    int st = configure(b.get(), logt, rb);
+    // the ring configuration when every member can run it (measured faster
+    // on the 64-lattice set), else the persistent kernel
+    bool ring = b->nrhs <= 65535u;
+    for (const tcp_mvp_plan *p : b->plans) ring = ring && p->nqubits >= kRingLogt;
+    int st = ring ? configure(b.get(), kRingLogt, 1) : TCP_ERR_INVALID_ARGUMENT;
+    if (st) st = configure(b.get(), logt, rb);
     if (st) {
         release_config(b.get());
         cudaStreamDestroy(b->capture_stream);
