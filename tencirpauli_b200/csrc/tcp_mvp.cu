@@ -1092,9 +1092,14 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     //    stream.  Pass k waits for part k only and runs the steps whose source
     //    tiles lie in it (the kernels' `pass`), adding to y after the first,
     //    so the copy of parts 1.. overlaps the earlier passes.
-    //  * Output: the last pass runs in kHostChunks launches over consecutive
-    //    output tiles; a third stream copies each finished chunk of y to the
-    //    host while the next chunk computes.
+    //  * Output: the first kFirstChunked passes run over every output tile;
+    //    the remaining ones run per chunk of kHostChunks consecutive output
+    //    tiles, all of a chunk's passes before the next chunk, and a third
+    //    stream copies each finished chunk of y to the host while the next
+    //    chunk computes.  Chunking the last two of four passes gives the
+    //    output copies half of the kernel time to overlap with (n = 28:
+    //    pageable 284 -> 257 ms, page-locked 261 -> 252 ms); chunking three
+    //    leaves the GPU waiting for the input staging.
     // Every launch is queued right after the copy it waits for; ordinary
     // (pageable) buffers move through the staging ring (HostCopies).  Smaller
     // applies copy, launch once and copy back on one stream.
@@ -1102,6 +1107,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     const uint64_t chunks = tiles >= kHostChunkTiles ? kHostChunks : 1;
     const bool passes = chunks > 1 && has_passes(plan, ws.x);
     constexpr int kParts = static_cast<int>(kPassChunks);
+    constexpr int kFirstChunked = kParts - 2;  // passes run per output chunk from here on
     cudaStream_t copy_stream = nullptr, in_stream = nullptr;
     cudaEvent_t done[kHostChunks] = {};
     cudaEvent_t landed[kParts] = {};
@@ -1124,7 +1130,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
                     if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, landed[k], 0);
                     if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
                 }
-                if (!status && k < kParts - 1) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
+                if (!status && k < kFirstChunked) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
             }
         } else {
             status = copies.to_device(ws.x, state, bytes, stream);
@@ -1132,8 +1138,12 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         const uint64_t per = tiles / chunks;
         for (uint64_t c = 0; c < chunks && !status; ++c) {
             const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
-            status = passes ? launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, kParts - 1, true)
-                            : launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
+            if (passes) {
+                for (int k = kFirstChunked; k < kParts && !status; ++k)
+                    status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, k, k > 0);
+            } else {
+                status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
+            }
             if (!status) {
                 e = cudaEventRecord(done[c], stream);
                 if (e != cudaSuccess) status = cuda_fail(e, "chunk event");
