@@ -90,6 +90,24 @@ int tcp_mlp_forward(const float *d_X, uint32_t count, const float *d_params, flo
 int tcp_mlp_backward_step(const float *d_X, const float *d_dc, uint32_t count, float *d_params, float *d_m,
                           float *d_v, float *d_work, float lr, uint32_t step, float *d_grad_out, void *stream);
 
+/* Scratch bytes for tcp_mlp_alignment_grad: six doubles per training set. */
+size_t tcp_mlp_alignment_work_bytes(uint32_t nsets);
+
+/* Derivative of the alignment objective with respect to the network outputs.
+ * Training set s covers states [d_seg_begin[s], d_seg_begin[s + 1]) (d_seg
+ * holds each state's set index).  Per state: network output d_c, denominator
+ * d_den (H_ii - theta), alpha = conj(e_i) r_i and gamma = conj(u_i) r_i
+ * (complex128), a = |r_i|^2; per set: E = ||e||^2, with r the residual, u the
+ * Ritz vector and e the direction Davidson is missing.  With
+ * g = -exp(clamp(c)) / den, A = sum g alpha, B = sum g^2 a, C = sum g gamma,
+ * the set's loss is 1 - |A|^2 / (E (B - |C|^2)), the objective their mean.
+ * Writes dL/dc to d_dc (zero where the clamp is active) and, if d_loss is
+ * non-null, the objective to d_loss[0].  Sums are reduced in a fixed order. */
+int tcp_mlp_alignment_grad(const float *d_c, const float *d_den, const void *d_alpha, const double *d_a,
+                           const void *d_gamma, const double *d_E, const int64_t *d_seg, const uint64_t *d_seg_begin,
+                           uint32_t nsets, uint64_t count, float clamp, double *d_work, float *d_dc, double *d_loss,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif

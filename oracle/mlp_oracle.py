@@ -157,3 +157,39 @@ def jacobi(diag: np.ndarray, r: np.ndarray, theta: float, eps: float = 1e-8) -> 
     d = diag.real - theta
     den = np.where(np.abs(d) < eps, np.where(d < 0, -eps, eps), d)
     return -r / den
+
+
+def alignment_loss(c, den, alpha, a, gamma, E, seg, nsets: int, clamp: float = 4.0) -> float:
+    """Alignment objective of the preconditioner's training: the mean over
+    training sets of 1 - |A|^2 / (E (B - |C|^2)) with g = -exp(clip(c)) / den,
+    A = sum g alpha, B = sum g^2 a, C = sum g gamma over the set's states."""
+    g = -np.exp(np.clip(np.asarray(c, np.float64), -clamp, clamp)) / np.asarray(den, np.float64)
+    A = np.zeros(nsets, np.complex128)
+    B = np.zeros(nsets)
+    C = np.zeros(nsets, np.complex128)
+    np.add.at(A, seg, g * alpha)
+    np.add.at(B, seg, g * g * a)
+    np.add.at(C, seg, g * gamma)
+    D = np.maximum(B - np.abs(C) ** 2, 1e-300)
+    return float(np.mean(1.0 - np.abs(A) ** 2 / (E * D)))
+
+
+def alignment_loss_and_dc(c, den, alpha, a, gamma, E, seg, nsets: int, clamp: float = 4.0) -> Tuple[float, np.ndarray]:
+    """The objective and its derivative with respect to each network output
+    (zero where the clip is active), by the chain rule through g."""
+    c = np.asarray(c, np.float64)
+    g = -np.exp(np.clip(c, -clamp, clamp)) / np.asarray(den, np.float64)
+    A = np.zeros(nsets, np.complex128)
+    B = np.zeros(nsets)
+    C = np.zeros(nsets, np.complex128)
+    np.add.at(A, seg, g * alpha)
+    np.add.at(B, seg, g * g * a)
+    np.add.at(C, seg, g * gamma)
+    D = np.maximum(B - np.abs(C) ** 2, 1e-300)
+    A2 = np.abs(A) ** 2
+    loss = float(np.mean(1.0 - A2 / (E * D)))
+    dA2 = 2.0 * np.real(np.conj(A[seg]) * alpha)
+    dD = 2.0 * g * a - 2.0 * np.real(np.conj(C[seg]) * gamma)
+    dLdg = -(dA2 * D[seg] - A2[seg] * dD) / (E[seg] * D[seg] ** 2) / nsets
+    inside = (c > -clamp) & (c < clamp)
+    return loss, np.where(inside, dLdg * g, 0.0)

@@ -87,6 +87,8 @@ SOLVER_SYMBOLS = (
     "tcp_mlp_train_step",
     "tcp_mlp_forward",
     "tcp_mlp_backward_step",
+    "tcp_mlp_alignment_work_bytes",
+    "tcp_mlp_alignment_grad",
 )
 
 
@@ -221,6 +223,9 @@ def load_library() -> ctypes.CDLL:
         lib.tcp_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp, vp]
         lib.tcp_mlp_forward.argtypes = [vp, u32, vp, vp, vp]
         lib.tcp_mlp_backward_step.argtypes = [vp, vp, u32, vp, vp, vp, vp, flt, u32, vp, vp]
+        lib.tcp_mlp_alignment_work_bytes.argtypes = [u32]
+        lib.tcp_mlp_alignment_work_bytes.restype = ctypes.c_size_t
+        lib.tcp_mlp_alignment_grad.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, u32, u64, flt, vp, vp, vp, vp]
         lib.tcp_u1_dimension.argtypes = [u32, u32, u64p]
         lib.tcp_u1_rank_words.argtypes = [u32, u32, u64p, u32, u64p]
         lib.tcp_u1_unrank_words.argtypes = [u32, u32, u64, u64p, u32]

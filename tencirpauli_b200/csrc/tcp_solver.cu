@@ -733,6 +733,92 @@ __global__ void k_mlp_inputs(const float *__restrict__ feat, const uint64_t *__r
     }
 }
 
+// ---------------------- alignment objective of the training ---------------------
+// A training set s covers the states [seg_begin[s], seg_begin[s + 1]).  With
+// g = -exp(clamp(c)) / den per state its sums are A = sum g alpha, B = sum g^2 a,
+// C = sum g gamma, D = max(B - |C|^2, 1e-300), and its loss is
+// 1 - |A|^2 / (E_s D): one minus the squared cosine between the correction
+// g o r, made orthogonal to the Ritz vector, and the missing direction.  The
+// objective is the mean over the sets.
+constexpr int kAlignThreads = 256;
+constexpr int kAlignWords = 6;  // A (2), B, C (2), loss per set
+
+__device__ __forceinline__ double align_g(float c, float den, float clamp) {
+    const double cc = fmin(fmax(static_cast<double>(c), -static_cast<double>(clamp)), static_cast<double>(clamp));
+    return -exp(cc) / static_cast<double>(den);
+}
+
+// One block per set; a fixed-order tree reduction, so the sums do not depend
+// on scheduling.
+__global__ void __launch_bounds__(kAlignThreads)
+    k_align_sums(const float *__restrict__ c, const float *__restrict__ den, const double2 *__restrict__ alpha,
+                 const double *__restrict__ a, const double2 *__restrict__ gamma, const double *__restrict__ E,
+                 const uint64_t *__restrict__ seg_begin, float clamp, double *__restrict__ sums) {
+    __shared__ double red[5][kAlignThreads];
+    const uint32_t s = blockIdx.x, t = threadIdx.x;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0, v4 = 0.0;
+    for (uint64_t i = seg_begin[s] + t; i < seg_begin[s + 1]; i += kAlignThreads) {
+        const double g = align_g(c[i], den[i], clamp);
+        const double2 al = alpha[i], ga = gamma[i];
+        v0 += g * al.x;
+        v1 += g * al.y;
+        v2 += g * g * a[i];
+        v3 += g * ga.x;
+        v4 += g * ga.y;
+    }
+    red[0][t] = v0;
+    red[1][t] = v1;
+    red[2][t] = v2;
+    red[3][t] = v3;
+    red[4][t] = v4;
+    __syncthreads();
+    for (uint32_t stride = kAlignThreads / 2; stride > 0; stride >>= 1) {
+        if (t < stride) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) red[k][t] += red[k][t + stride];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        double *q = sums + static_cast<size_t>(s) * kAlignWords;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) q[k] = red[k][0];
+        const double D = fmax(red[2][0] - (red[3][0] * red[3][0] + red[4][0] * red[4][0]), 1e-300);
+        const double A2 = red[0][0] * red[0][0] + red[1][0] * red[1][0];
+        q[5] = 1.0 - A2 / (E[s] * D);
+    }
+}
+
+// dL/dc per state (zero where the clamp is active).
+__global__ void k_align_dc(const float *__restrict__ c, const float *__restrict__ den, const double2 *__restrict__ alpha,
+                           const double *__restrict__ a, const double2 *__restrict__ gamma, const double *__restrict__ E,
+                           const int64_t *__restrict__ seg, uint64_t count, uint32_t nsets, float clamp,
+                           const double *__restrict__ sums, float *__restrict__ dc) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const int64_t s = seg[i];
+        const double *q = sums + static_cast<size_t>(s) * kAlignWords;
+        const double D = fmax(q[2] - (q[3] * q[3] + q[4] * q[4]), 1e-300);
+        const double A2 = q[0] * q[0] + q[1] * q[1];
+        const double g = align_g(c[i], den[i], clamp);
+        const double2 al = alpha[i], ga = gamma[i];
+        const double dA2 = 2.0 * (q[0] * al.x + q[1] * al.y);
+        const double dD = 2.0 * g * a[i] - 2.0 * (q[3] * ga.x + q[4] * ga.y);
+        const double dLdg = -(dA2 * D - A2 * dD) / (E[s] * D * D) / static_cast<double>(nsets);
+        const float ci = c[i];
+        dc[i] = (ci > -clamp && ci < clamp) ? static_cast<float>(dLdg * g) : 0.f;
+    }
+}
+
+// Mean of the per-set losses, summed in set order.
+__global__ void k_align_loss(const double *__restrict__ sums, uint32_t nsets, double *__restrict__ loss) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double l = 0.0;
+        for (uint32_t s = 0; s < nsets; ++s) l += sums[static_cast<size_t>(s) * kAlignWords + 5];
+        *loss = l / static_cast<double>(nsets);
+    }
+}
+
 int grid_for(uint64_t n, int threads) {
     return static_cast<int>(std::min<uint64_t>((n + threads - 1) / threads, 148ull * 16));
 }
@@ -1020,4 +1106,30 @@ extern "C" int tcp_mlp_train_step(const float *d_X, const float *d_den, const fl
     if (d_loss_out) k_sum_losses<<<1, 32, 0, s>>>(loss_partial, TCP_MLP_TRAIN_BLOCKS, d_loss_out);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? TCP_OK : cuda_fail(e, "mlp training launch");
+}
+
+extern "C" size_t tcp_mlp_alignment_work_bytes(uint32_t nsets) {
+    return static_cast<size_t>(nsets) * kAlignWords * sizeof(double);
+}
+
+extern "C" int tcp_mlp_alignment_grad(const float *d_c, const float *d_den, const void *d_alpha, const double *d_a,
+                                      const void *d_gamma, const double *d_E, const int64_t *d_seg,
+                                      const uint64_t *d_seg_begin, uint32_t nsets, uint64_t count, float clamp,
+                                      double *d_work, float *d_dc, double *d_loss, void *stream) {
+    if (!d_c || !d_den || !d_alpha || !d_a || !d_gamma || !d_E || !d_seg || !d_seg_begin || !d_work || !d_dc) {
+        return fail(TCP_ERR_INVALID_ARGUMENT, "null buffer");
+    }
+    if (nsets == 0) return fail(TCP_ERR_INVALID_ARGUMENT, "the alignment objective needs at least one set");
+    if (!(clamp > 0.f)) return fail(TCP_ERR_INVALID_ARGUMENT, "clamp must be positive");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_align_sums<<<nsets, kAlignThreads, 0, s>>>(d_c, d_den, static_cast<const double2 *>(d_alpha), d_a,
+                                                 static_cast<const double2 *>(d_gamma), d_E, d_seg_begin, clamp, d_work);
+    if (count > 0) {
+        k_align_dc<<<grid_for(count, 256), 256, 0, s>>>(d_c, d_den, static_cast<const double2 *>(d_alpha), d_a,
+                                                       static_cast<const double2 *>(d_gamma), d_E, d_seg, count, nsets,
+                                                       clamp, d_work, d_dc);
+    }
+    if (d_loss) k_align_loss<<<1, 32, 0, s>>>(d_work, nsets, d_loss);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TCP_OK : cuda_fail(e, "alignment gradient launch");
 }

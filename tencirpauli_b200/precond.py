@@ -257,6 +257,7 @@ class AlignmentSets:
     E: Any  # (S,) float64: ||e||^2 per set
     seg: Any  # (N,) int64 set index
     nsets: int
+    seg_begin: Any = None  # (S + 1,) int64 offsets of the sets (contiguous)
 
 
 def _cat_alignment(parts: Sequence[AlignmentSets]) -> AlignmentSets:
@@ -276,7 +277,19 @@ def _cat_alignment(parts: Sequence[AlignmentSets]) -> AlignmentSets:
         E=torch.cat([p.E for p in parts]),
         seg=torch.cat(segs),
         nsets=offset,
+        seg_begin=_offsets(torch.cat(segs), offset),
     )
+
+
+def _offsets(seg: Any, nsets: int) -> Any:
+    """Offsets of the sets; the states of a set must be contiguous."""
+    import torch
+
+    if seg.numel() > 1 and not bool(torch.all(seg[1:] >= seg[:-1])):
+        raise ValueError("alignment training sets must be contiguous (set index non-decreasing)")
+    begin = torch.zeros(nsets + 1, dtype=torch.int64, device=seg.device)
+    begin[1:] = torch.cumsum(torch.bincount(seg, minlength=nsets), 0)
+    return begin
 
 
 def collect_alignment_sets(
@@ -340,42 +353,31 @@ def collect_alignment_sets(
     return _cat_alignment(parts) if parts else None
 
 
-def alignment_loss_and_dc(c: Any, data: AlignmentSets, clamp: float = 4.0):
-    """Mean alignment loss over the sets and dL/dc per basis state."""
-    import torch
-
-    S = data.nsets
-    cc = torch.clamp(c.double(), -clamp, clamp)
-    g = -torch.exp(cc) / data.den.double()
-    A = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add_(0, data.seg, g * data.alpha)
-    B = torch.zeros(S, dtype=torch.float64, device="cuda").index_add_(0, data.seg, g * g * data.a)
-    C = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add_(0, data.seg, g * data.gamma)
-    D = torch.clamp(B - C.abs() ** 2, min=1e-300)
-    A2 = A.abs() ** 2
-    loss = torch.mean(1.0 - A2 / (data.E * D))
-    As, Cs, Ds, Es, A2s = A[data.seg], C[data.seg], D[data.seg], data.E[data.seg], A2[data.seg]
-    dA2 = 2.0 * (torch.conj(As) * data.alpha).real
-    dD = 2.0 * g * data.a - 2.0 * (torch.conj(Cs) * data.gamma).real
-    dLdg = -(dA2 * Ds - A2s * dD) / (Es * Ds * Ds) / S
-    inside = (c.double() > -clamp) & (c.double() < clamp)
-    dc = torch.where(inside, dLdg * g, torch.zeros_like(g))
-    return float(loss), dc.float()
+def alignment_loss_and_dc(c: Any, data: AlignmentSets, clamp: float = 4.0, work: Any = None):
+    """Mean alignment loss over the sets and dL/dc per basis state, from the
+    device kernels of tcp_mlp_alignment_grad (per-set sums in a fixed order,
+    then the elementwise derivative)."""
+    seg_begin = data.seg_begin if data.seg_begin is not None else _offsets(data.seg, data.nsets)
+    return solver_ops.alignment_grad(c, data.den, data.alpha, data.a, data.gamma, data.E, data.seg, seg_begin, clamp,
+                                     work=work)
 
 
 def train_alignment(
     data: AlignmentSets, params: Optional[np.ndarray] = None, steps: int = 300, lr: float = 3e-3, seed: int = 0, log_every: int = 50
 ) -> Tuple[np.ndarray, List[float]]:
-    """Adam on the alignment loss: forward and backward through the device
-    kernels (tcp_mlp_forward, tcp_mlp_backward_step); the loss-level
-    derivative dL/dc is elementwise GPU arithmetic."""
+    """Adam on the alignment loss, every step on the device kernels:
+    tcp_mlp_forward, tcp_mlp_alignment_grad (the loss and dL/dc) and
+    tcp_mlp_backward_step (back-propagation and the Adam update)."""
     import torch
 
     p = torch.from_numpy(init_params(seed) if params is None else np.asarray(params, np.float32)).cuda()
     trainer = solver_ops.MLPTrainer(p)
+    work = torch.empty(int(solver_ops._lib().tcp_mlp_alignment_work_bytes(data.nsets)) // 8, dtype=torch.float64,
+                       device="cuda")
     losses: List[float] = []
     for s in range(steps):
         c = solver_ops.mlp_forward(data.X, p)
-        loss, dc = alignment_loss_and_dc(c, data)
+        loss, dc = alignment_loss_and_dc(c, data, work=work)
         trainer.backward_step(data.X, dc, lr)
         if s % log_every == 0 or s == steps - 1:
             losses.append(loss)

@@ -8,7 +8,7 @@ reduction and combination runs in FP64 on the device.
 from __future__ import annotations
 
 import ctypes
-from typing import Any
+from typing import Any, Tuple
 
 from . import _native
 
@@ -183,6 +183,35 @@ def mlp_forward(X: Any, params: Any, out: Any = None, stream: Any = None) -> Any
         out = torch.empty(count, dtype=torch.float32, device="cuda")
     _native.raise_for_status(_lib().tcp_mlp_forward(_ptr(X), count, _ptr(params), _ptr(out), _stream(stream)))
     return out
+
+
+def alignment_grad(c: Any, den: Any, alpha: Any, a: Any, gamma: Any, E: Any, seg: Any, seg_begin: Any, clamp: float,
+                   work: Any = None, dc: Any = None, stream: Any = None) -> Tuple[float, Any]:
+    """(objective, dL/dc) of the alignment objective (tcp_mlp_alignment_grad):
+    float32 c and den, complex128 alpha and gamma, float64 a per state; float64
+    E per set; int64 set index per state and int64 set offsets (nsets + 1)."""
+    import torch
+
+    nsets = int(E.shape[0])
+    count = int(c.shape[0])
+    for t, dt in ((c, torch.float32), (den, torch.float32), (alpha, torch.complex128), (a, torch.float64),
+                  (gamma, torch.complex128), (E, torch.float64), (seg, torch.int64), (seg_begin, torch.int64)):
+        if t.dtype != dt or not t.is_contiguous() or t.device.type != "cuda":
+            raise ValueError("alignment inputs must be contiguous CUDA tensors of the documented dtypes")
+    if seg_begin.shape[0] != nsets + 1 or any(int(t.shape[0]) != count for t in (den, alpha, a, gamma, seg)):
+        raise ValueError("alignment inputs have inconsistent lengths")
+    if work is None or work.numel() * 8 < int(_lib().tcp_mlp_alignment_work_bytes(nsets)):
+        work = torch.empty(int(_lib().tcp_mlp_alignment_work_bytes(nsets)) // 8, dtype=torch.float64, device="cuda")
+    if dc is None:
+        dc = torch.empty(count, dtype=torch.float32, device="cuda")
+    loss = torch.empty(1, dtype=torch.float64, device="cuda")
+    _native.raise_for_status(
+        _lib().tcp_mlp_alignment_grad(
+            _ptr(c), _ptr(den), _ptr(alpha), _ptr(a), _ptr(gamma), _ptr(E), _ptr(seg), _ptr(seg_begin), nsets, count,
+            float(clamp), _ptr(work), _ptr(dc), _ptr(loss), _stream(stream),
+        )
+    )
+    return float(loss.item()), dc
 
 
 class MLPTrainer:

@@ -222,7 +222,7 @@ def test_alignment_gradient_matches_autograd_and_forward_matches_oracle() -> Non
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     n, S = 4000, 3
-    seg = torch.arange(n, device="cuda") % S
+    seg = (torch.arange(n, device="cuda") * S) // n  # contiguous sets, as the training data lays them out
     c = 0.3 * torch.randn(n, device="cuda", dtype=torch.float64, generator=g)
     den = (torch.rand(n, device="cuda", generator=g, dtype=torch.float64) + 0.5).float()
     r = _rand((n,), torch.complex128, 11)
@@ -240,7 +240,7 @@ def test_alignment_gradient_matches_autograd_and_forward_matches_oracle() -> Non
     C = torch.zeros(S, dtype=torch.complex128, device="cuda").index_add(0, seg, gg * data.gamma)
     ref = torch.mean(1 - A.abs() ** 2 / (E * (B - C.abs() ** 2)))
     ref.backward()
-    assert abs(loss - float(ref.detach())) <= 1e-10
+    assert abs(loss - float(ref.detach())) <= 1e-12
     np.testing.assert_allclose(dc.cpu().numpy(), cv.grad.cpu().numpy(), rtol=1e-4, atol=1e-9)
     # device forward pass against the NumPy restatement
     params = np.random.default_rng(5).normal(scale=0.4, size=mo.NPARAM).astype(np.float32)
@@ -248,3 +248,29 @@ def test_alignment_gradient_matches_autograd_and_forward_matches_oracle() -> Non
     out = solver_ops.mlp_forward(torch.from_numpy(X).cuda(), torch.from_numpy(params).cuda()).cpu().numpy()
     ref_c, _ = mo.forward(params.astype(np.float64), X.astype(np.float64))
     np.testing.assert_allclose(out, ref_c, rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("sizes", [(40, 25, 57), (70001, 3, 65536, 1000)])
+def test_alignment_gradient_kernel_matches_oracle(sizes) -> None:
+    from test_mlp_oracle_cpu import alignment_data
+
+    c, den, alpha, a, gamma, E, seg, S = alignment_data(seed=11, sizes=sizes)
+    c32, den32 = c.astype(np.float32), den.astype(np.float32)
+    want_loss, want_dc = mo.alignment_loss_and_dc(c32, den32, alpha, a, gamma, E, seg, S)
+    seg_t = torch.from_numpy(seg.astype(np.int64)).cuda()
+    begin = torch.from_numpy(np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)).cuda()
+    cuda = lambda v, dt: torch.from_numpy(np.ascontiguousarray(v)).to(dt).cuda()  # noqa: E731
+    loss, dc = solver_ops.alignment_grad(
+        cuda(c32, torch.float32), cuda(den32, torch.float32), cuda(alpha, torch.complex128), cuda(a, torch.float64),
+        cuda(gamma, torch.complex128), cuda(E, torch.float64), seg_t, begin, 4.0,
+    )
+    assert abs(loss - want_loss) <= 1e-12 * max(1.0, abs(want_loss))
+    got = dc.cpu().numpy().astype(np.float64)
+    np.testing.assert_allclose(got, want_dc, rtol=1e-5, atol=1e-6 * np.abs(want_dc).max())
+    assert np.all(got[c32 >= 4.0] == 0.0)
+    # the same sums in the same order: a second call is bit-identical
+    loss2, dc2 = solver_ops.alignment_grad(
+        cuda(c32, torch.float32), cuda(den32, torch.float32), cuda(alpha, torch.complex128), cuda(a, torch.float64),
+        cuda(gamma, torch.complex128), cuda(E, torch.float64), seg_t, begin, 4.0,
+    )
+    assert loss2 == loss and torch.equal(dc2, dc)
