@@ -521,6 +521,12 @@ __device__ __forceinline__ void mlp_inputs(const float *__restrict__ f, double t
     x[7] = static_cast<float>(ratio / (1.0 + ratio));
 }
 
+// tanh(a) = 1 - 2 / (exp(2a) + 1), an exact identity, evaluated with the
+// fast exponential and division intrinsics: a handful of instructions, about
+// 1e-7 absolute error (all the activations need), and it saturates to +-1 for
+// large |a| (the exponential overflows to inf or underflows to 0).
+__device__ __forceinline__ float act_tanh(float a) { return 1.f - __fdividef(2.f, __expf(2.f * a) + 1.f); }
+
 __device__ __forceinline__ float mlp_forward(const float *__restrict__ w, const float (&x)[IN], float (&h1)[HID],
                                              float (&h2)[HID]) {
 #pragma unroll 4
@@ -528,18 +534,42 @@ __device__ __forceinline__ float mlp_forward(const float *__restrict__ w, const 
         float a = w[OFF_B1 + o];
 #pragma unroll
         for (int i = 0; i < IN; ++i) a = fmaf(w[OFF_W1 + o * IN + i], x[i], a);
-        h1[o] = tanhf(a);
+        h1[o] = act_tanh(a);
     }
 #pragma unroll 4
     for (int o = 0; o < HID; ++o) {
         float a = w[OFF_B2 + o];
 #pragma unroll 8
         for (int i = 0; i < HID; ++i) a = fmaf(w[OFF_W2 + o * HID + i], h1[i], a);
-        h2[o] = tanhf(a);
+        h2[o] = act_tanh(a);
     }
     float c = w[OFF_B3];
 #pragma unroll 8
     for (int i = 0; i < HID; ++i) c = fmaf(w[OFF_W3 + i], h2[i], c);
+    return c;
+}
+
+// Network output c for one input row without the activations: layer 1 is
+// evaluated unit by unit with the layer-2 sums accumulated alongside, so no
+// activation array is indexed at run time (mlp_forward's arrays, indexed in
+// partly unrolled loops, live in local memory).  The same operations in the
+// same order as mlp_forward, so the output is identical.
+__device__ __forceinline__ float mlp_eval(const float *__restrict__ w, const float (&x)[IN]) {
+    float a2[HID];
+#pragma unroll
+    for (int p = 0; p < HID; ++p) a2[p] = w[OFF_B2 + p];
+#pragma unroll 2
+    for (int o = 0; o < HID; ++o) {
+        float a = w[OFF_B1 + o];
+#pragma unroll
+        for (int i = 0; i < IN; ++i) a = fmaf(w[OFF_W1 + o * IN + i], x[i], a);
+        const float h = act_tanh(a);
+#pragma unroll
+        for (int p = 0; p < HID; ++p) a2[p] = fmaf(w[OFF_W2 + p * HID + o], h, a2[p]);
+    }
+    float c = w[OFF_B3];
+#pragma unroll
+    for (int p = 0; p < HID; ++p) c = fmaf(w[OFF_W3 + p], act_tanh(a2[p]), c);
     return c;
 }
 
@@ -557,17 +587,17 @@ __global__ void k_mlp_precond(const void *__restrict__ R, int r64, uint64_t n, u
         const float *f = feat + r * TCP_FEATURES;
         const double d = diag[r].x;
         for (uint32_t j = 0; j < k; ++j) {
-            float x[IN], h1[HID], h2[HID];
+            float x[IN];
             double den_f;
             mlp_inputs(f, theta[j], scale, eps, x, den_f);
             double den = d - theta[j];
             if (fabs(den) < eps) den = den < 0.0 ? -eps : eps;
-            const float c = fminf(fmaxf(mlp_forward(w, x, h1, h2), -clamp), clamp);
+            const float c = fminf(fmaxf(mlp_eval(w, x), -clamp), clamp);
             const double2 v = load_c(R, r64, j * n + r);
             if (c == 0.f) {  // the Jacobi correction, rounded exactly as k_jacobi
                 store_c(T, t64, j * n + r, make_double2(-v.x / den, -v.y / den));
             } else {
-                const double g = -exp(static_cast<double>(c)) / den;
+                const double g = -static_cast<double>(__expf(c)) / den;  // |c| <= clamp
                 store_c(T, t64, j * n + r, make_double2(g * v.x, g * v.y));
             }
         }
@@ -694,10 +724,10 @@ __global__ void k_mlp_forward(const float *__restrict__ X, uint32_t count, const
     for (int e = threadIdx.x; e < NPARAM; e += blockDim.x) w[e] = wglob[e];
     __syncthreads();
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
-        float x[IN], h1[HID], h2[HID];
+        float x[IN];
 #pragma unroll
         for (int i = 0; i < IN; ++i) x[i] = X[static_cast<size_t>(s) * IN + i];
-        out[s] = mlp_forward(w, x, h1, h2);
+        out[s] = mlp_eval(w, x);
     }
 }
 
