@@ -68,6 +68,40 @@ def _profile_traffic(kernel: str) -> Optional[float]:
     return None
 
 
+def _profile_instructions(kernel: str, workload: str) -> Optional[float]:
+    """Warp instructions per launch (smsp__inst_executed.sum) from the
+    committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "instructions.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+def _issue_roofline(kernel: str, workload: str, kernel_ms: float, clocks: Dict[str, Any]) -> Optional[Dict[str, Any]]:
+    """Instruction-issue ceiling: an SM issues at most one warp instruction
+    per clock on each of its 4 schedulers.  Achieved = the kernel's warp
+    instructions per launch (ncu, committed) over the CUDA-event launch time;
+    peak = 4 x SMs x the median SM clock sampled during the timed region."""
+    import torch
+
+    inst = _profile_instructions(kernel, workload)
+    mhz = clocks.get("sm_mhz") if isinstance(clocks, dict) else None
+    if inst is None or not mhz:
+        return None
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    peak = 4.0 * sms * float(mhz) * 1e6
+    achieved = inst / (kernel_ms / 1000.0)
+    return {"achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "T warp-instructions/s", "frac": achieved / peak,
+            "instructions_per_launch": inst, "source": "profiles/instructions.txt (ncu smsp__inst_executed.sum)"}
+
+
 def manifest(with_gpu: bool = True) -> Dict[str, Any]:
     """What produced a bench line: the library's build record (source commit,
     nvcc release), a digest of the sources as they ran, host core count,
@@ -669,6 +703,21 @@ def run_sector(args: argparse.Namespace) -> None:
     peaks = _measured_peaks()
     b_alg = dim * (4 + 16 + 2 * elem)  # basis word, diagonal, x, y
     achieved = b_alg / (ms / 1e3) / 1e9
+    # k_u1_apply is bound by instruction issue (gathers and table lookups
+    # in flight, not bytes): its roofline is the issue rate, with the
+    # compulsory HBM bytes beside it
+    hbm = {"achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+           "bytes_per_launch": b_alg, "peak_source": peaks["source"]}
+    issue = _issue_roofline("k_u1_apply", f"j1j2_{lx}x{ly}_half_{args.dtype}", ms, clocks)
+    if issue is not None:
+        sector_roofline = dict(bound="issue", **{k: issue[k] for k in ("achieved", "peak", "unit", "frac")},
+                               kernel="k_u1_apply", kernel_ms=ms, instructions_per_launch=issue["instructions_per_launch"],
+                               peak_source="4 warp instructions per SM clock x SMs x sampled SM clock; "
+                               + issue["source"], hbm=hbm)
+    else:
+        sector_roofline = dict(bound="issue (instruction count not profiled for this lattice; HBM shown)",
+                               **{k: hbm[k] for k in ("achieved", "peak", "unit", "frac")}, kernel="k_u1_apply",
+                               kernel_ms=ms, bytes_per_launch=b_alg, peak_source=peaks["source"])
     line = {
         "metric": "Sector MVP amplitude-terms/s",
         "value": value,
@@ -685,10 +734,7 @@ def run_sector(args: argparse.Namespace) -> None:
         "config": {"workload": f"periodic {lx}x{ly} J1-J2 (J1=1, J2=0.5), half-filling U(1) sector", "nqubits": n,
                    "particle_number": k, "dimension": dim, "terms": T, "groups": native.group_count,
                    "l2": f"restricted state {dim * 16 / 1e6:.0f} MB" + ("; > L2, no flush needed" if dim * 16 > 126e6 else "; fits in L2")},
-        "roofline": {"bound": "issue (integer/FP64 instruction rate; HBM bytes shown for reference)",
-                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "kernel": "k_u1_apply", "bytes_per_launch": b_alg,
-                     "kernel_ms": ms, "peak_source": peaks["source"]},
+        "roofline": sector_roofline,
         "e2e": {"value": T * dim / e2e_s, "unit": UNIT, "h2d_bytes_per_step": dim * 16, "d2h_bytes_per_step": dim * 16,
                 "ms_per_step": 1e3 * e2e_s},
         "gpu_launches": args.steps,
@@ -1083,6 +1129,7 @@ def main() -> None:
                     "flops_per_launch": f_alg,
                     "peak_source": "tcp_probe_fma_rate: FMA chains on every SM of this GPU, best of 5",
                 },
+                "issue": _issue_roofline(kernel_name, f"random{args.words}_n{n}", kern_ms, clocks),
                 "hbm": {
                     "achieved": achieved,
                     "peak": peaks["hbm_gbs"],
