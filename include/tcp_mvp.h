@@ -193,12 +193,19 @@ int tcp_mvp_apply_add_device(const tcp_mvp_plan *plan, const void *d_state, void
  * Every member needs at least 8 qubits.  The batch keeps pointers to its plans,
  * which must outlive it.  Work items are (member, tile of 2^tile_rows_log2
  * rows, block of rhs_block vectors), largest member first.
+ * The ring configuration (tile_rows_log2 = 12, rhs_block = 1; the default
+ * when every member has at least 12 qubits) instead records one ring-kernel
+ * launch per member with a term, over all its tiles and all nrhs vectors
+ * (nrhs <= 65535), in the same graph; its graph captures the buffers, so it
+ * is rebuilt when they change.  tcp_mvp_batch_info then reports the total
+ * CTAs as `items` and the number of launches as `grid`.
  */
 typedef struct tcp_mvp_batch tcp_mvp_batch;
 int tcp_mvp_batch_create(uint32_t count, const tcp_mvp_plan *const *plans, uint32_t nrhs, int dtype,
                          tcp_mvp_batch **out_batch);
 int tcp_mvp_batch_destroy(tcp_mvp_batch *batch);
-/* Choose the tile rows (2^8..2^10) and RHS block (1, 2, 4, 8; divides nrhs). */
+/* Choose the tile rows (2^8..2^10) and RHS block (1, 2, 4, 8; divides nrhs),
+ * or the ring configuration (12, 1). */
 int tcp_mvp_batch_configure(tcp_mvp_batch *batch, uint32_t tile_rows_log2, uint32_t rhs_block);
 /* Time every kernel variant on these buffers (`repeats` launches each) and keep
  * the fastest; with a non-empty cache_path the choice is read from / appended
