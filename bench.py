@@ -881,6 +881,27 @@ def run_sharded(args: argparse.Namespace, world: int, rank: int) -> None:
     dots = torch.stack([torch.vdot(a, y), torch.vdot(ha, x)]).to(torch.complex128)
     dist.all_reduce(dots)
     herm = abs(complex(dots[0]) - complex(dots[1])) / max(abs(complex(dots[0])), 1e-300)
+    # Ceilings of one step per rank: instruction issue for the applies (the
+    # single-GPU launch's committed instruction count split evenly over the
+    # ranks, an estimate: the per-pattern plans are not the full plan) and
+    # NVLink for the exchanges (one shard per nonzero top pattern received,
+    # against the 770 GB/s per direction measured for a peer copy on this
+    # pool).  The step time covers both, so both achieved rates are lower
+    # bounds.
+    step_s = ms_per_step / 1000.0
+    recv_bytes = len(mvp.patterns) * mvp.shard_len * elem
+    nvlink = {"achieved": recv_bytes / step_s / 1e9, "peak": 770.0, "unit": "GB/s",
+              "frac": recv_bytes / step_s / 770e9, "bytes_per_rank_per_step": recv_bytes,
+              "peak_source": "peer copy measured on this pool, per direction"}
+    kernel_name = "k_ring<double>" if args.dtype == "c128" else "k_ring<float>"
+    issue = _issue_roofline(kernel_name, f"random{args.words}_n{n}", ms_per_step * world, clocks)
+    if issue is not None:
+        roofline = {"bound": "issue (estimated per rank)", **{k: issue[k] for k in ("achieved", "peak", "unit", "frac")},
+                    "traffic": None, "kernel": kernel_name,
+                    "note": "instructions of the single-GPU launch / ranks over the step time", "nvlink": nvlink}
+    else:
+        roofline = {"bound": "nvlink", **{k: nvlink[k] for k in ("achieved", "peak", "unit", "frac")}, "traffic": None,
+                    "kernel": kernel_name}
     line = {
         "metric": METRIC,
         "value": value,
@@ -901,6 +922,7 @@ def run_sharded(args: argparse.Namespace, world: int, rank: int) -> None:
                 "d2h_bytes_per_step": dim * elem, "ms_per_step": 1e3 * float(e2e_t.item()),
                 "note": "bytes summed over ranks; each rank copies its own shard"},
         "gpu_launches": args.steps * (len(mvp.patterns) + 1),
+        "roofline": roofline,
         "clocks": clocks,
         "accuracy": {"hermiticity_rel": herm},
         "manifest": manifest(),
@@ -1093,6 +1115,50 @@ def main() -> None:
         f_ach = f_alg / (kern_ms / 1000.0)
         smem_bytes = dim * (int(info.cosets) + int(info.ring_steps)) * elem
         smem_ach = smem_bytes / (kern_ms / 1000.0)
+        # The binding resource is instruction issue (the per-record integer
+        # chain ahead of the multiply-adds; ncu: issue active about half the
+        # cycles, neither the shared-memory nor the FMA pipe saturated), so
+        # the main roofline is the issue rate; shared memory, the FMA pipe
+        # and HBM are reported beside it.
+        smem_obj = {
+            "achieved": smem_ach / 1e12,
+            "peak": smem_rate / 1e12,
+            "unit": "TB/s",
+            "frac": smem_ach / smem_rate,
+            "peak_source": "tcp_probe_smem_rate: 16-byte shared-memory reads in the kernel's pattern on every SM "
+            "of this GPU, best of 5",
+            "bytes_per_launch": smem_bytes,
+            "units": f"2^{n} rows x ({int(info.cosets)} coset operands + {int(info.ring_steps)} tile fills) x {elem} B",
+        }
+        fp_obj = {
+            "achieved": f_ach / 1e12,
+            "peak": fma_rate / 1e12,
+            "unit": "TFLOP/s",
+            "frac": f_ach / fma_rate,
+            "flops_per_launch": f_alg,
+            "peak_source": "tcp_probe_fma_rate: FMA chains on every SM of this GPU, best of 5",
+        }
+        hbm_obj = {
+            "achieved": achieved,
+            "peak": peaks["hbm_gbs"],
+            "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"],
+            "bytes_per_launch": b_alg,
+            "peak_source": peaks["source"],
+            "traffic_gbs": (traffic / (kern_ms / 1000.0) / 1e9) if traffic else None,
+        }
+        issue_obj = _issue_roofline(kernel_name, f"random{args.words}_n{n}", kern_ms, clocks)
+        if issue_obj is not None:
+            ring_roofline = {"bound": "issue", **{k: issue_obj[k] for k in ("achieved", "peak", "unit", "frac")},
+                             "traffic": traffic, "kernel": kernel_name, "kernel_ms": kern_ms,
+                             "instructions_per_launch": issue_obj["instructions_per_launch"],
+                             "peak_source": "4 warp instructions per SM clock x SMs x sampled SM clock; " + issue_obj["source"],
+                             "smem": smem_obj, "fp": fp_obj, "hbm": hbm_obj}
+        else:  # no committed instruction count for this workload: shared memory leads
+            ring_roofline = {"bound": "smem", **{k: smem_obj[k] for k in ("achieved", "peak", "unit", "frac")},
+                             "traffic": traffic, "kernel": kernel_name, "kernel_ms": kern_ms,
+                             "peak_source": smem_obj["peak_source"], "smem_bytes_per_launch": smem_bytes,
+                             "fp": fp_obj, "hbm": hbm_obj}
         line = {
             "metric": METRIC,
             "value": value,
@@ -1107,39 +1173,7 @@ def main() -> None:
             "dtype": "f64" if args.dtype == "c128" else "f32",
             "data": "synthetic",
             "config": workload_config(args, op),
-            "roofline": {
-                "bound": "smem",
-                "achieved": smem_ach / 1e12,
-                "peak": smem_rate / 1e12,
-                "unit": "TB/s",
-                "frac": smem_ach / smem_rate,
-                "traffic": traffic,
-                "peak_source": "tcp_probe_smem_rate: 16-byte shared-memory reads in the kernel's pattern on every SM "
-                "of this GPU, best of 5",
-                "kernel": kernel_name,
-                "kernel_ms": kern_ms,
-                "smem_bytes_per_launch": smem_bytes,
-                "smem_units": f"2^{n} rows x ({int(info.cosets)} coset operands + {int(info.ring_steps)} tile fills) "
-                f"x {elem} B",
-                "fp": {
-                    "achieved": f_ach / 1e12,
-                    "peak": fma_rate / 1e12,
-                    "unit": "TFLOP/s",
-                    "frac": f_ach / fma_rate,
-                    "flops_per_launch": f_alg,
-                    "peak_source": "tcp_probe_fma_rate: FMA chains on every SM of this GPU, best of 5",
-                },
-                "issue": _issue_roofline(kernel_name, f"random{args.words}_n{n}", kern_ms, clocks),
-                "hbm": {
-                    "achieved": achieved,
-                    "peak": peaks["hbm_gbs"],
-                    "unit": "GB/s",
-                    "frac": achieved / peaks["hbm_gbs"],
-                    "bytes_per_launch": b_alg,
-                    "peak_source": peaks["source"],
-                    "traffic_gbs": (traffic / (kern_ms / 1000.0) / 1e9) if traffic else None,
-                },
-            },
+            "roofline": ring_roofline,
             "e2e": {
                 "value": e2e_value,
                 "unit": UNIT,
