@@ -597,7 +597,19 @@ int g_num_sms = 0;
 // Host apply at n = 28 (65,536 tiles): 4 input parts and 8 output chunks
 // measured 280 ms; 8 parts and 16 chunks measured 312 ms (more passes over
 // y and more pass start-up than the shorter exposed copies save).
-constexpr uint64_t kHostChunks = 8;         // output-tile chunks of a large host apply
+constexpr uint64_t kHostEqualChunks = 8;                  // output-tile chunks of a large host apply,
+constexpr uint64_t kHostChunks = kHostEqualChunks + 2;    // the last one split into 1/2, 1/4, 1/4
+
+// First output tile of chunk c (c = kHostChunks: the end): equal chunks, the
+// last of them split in a half and two quarters, so that the copy still to
+// do once the last kernel has finished is a quarter of an equal chunk.
+uint64_t chunk_start(uint64_t c, uint64_t tiles) {
+    const uint64_t per = tiles / kHostEqualChunks, last = (kHostEqualChunks - 1) * per;
+    if (c + 3 <= kHostChunks) return c * per;
+    if (c + 2 == kHostChunks) return last + per / 2;
+    if (c + 1 == kHostChunks) return last + 3 * per / 4;
+    return tiles;
+}
 constexpr uint64_t kHostChunkTiles = 8192;  // tiles from which the host apply is chunked
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -1093,10 +1105,11 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     //    tiles lie in it (the kernels' `pass`), adding to y after the first,
     //    so the copy of parts 1.. overlaps the earlier passes.
     //  * Output: the first kFirstChunked passes run over every output tile;
-    //    the remaining ones run per chunk of kHostChunks consecutive output
-    //    tiles, all of a chunk's passes before the next chunk, and a third
-    //    stream copies each finished chunk of y to the host while the next
-    //    chunk computes.  Chunking the last two of four passes gives the
+    //    the remaining ones run per chunk of consecutive output tiles
+    //    (chunk_start), all of a chunk's passes before the next chunk, and a
+    //    third stream copies each finished chunk of y to the host while the
+    //    next chunk computes.  The last chunks are smaller, so little copying
+    //    is left once the last kernel has finished (n = 28: 7-10 ms less).  Chunking the last two of four passes gives the
     //    output copies half of the kernel time to overlap with (n = 28:
     //    pageable 284 -> 257 ms, page-locked 261 -> 252 ms); chunking three
     //    leaves the GPU waiting for the input staging.
@@ -1135,9 +1148,9 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         } else {
             status = copies.to_device(ws.x, state, bytes, stream);
         }
-        const uint64_t per = tiles / chunks;
+        auto start = [&](uint64_t c) { return chunks == 1 ? (c ? tiles : 0) : chunk_start(c, tiles); };
         for (uint64_t c = 0; c < chunks && !status; ++c) {
-            const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
+            const uint64_t t0 = start(c), nt = start(c + 1) - t0;
             if (passes) {
                 for (int k = kFirstChunked; k < kParts && !status; ++k)
                     status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, k, k > 0);
@@ -1152,7 +1165,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
         const size_t row_bytes = 2 * sizeof(R);
         const uint64_t rows_per_tile = plan->dim / tiles;
         for (uint64_t c = 0; c < chunks && !status; ++c) {
-            const uint64_t t0 = c * per, nt = (c + 1 == chunks) ? tiles - t0 : per;
+            const uint64_t t0 = start(c), nt = start(c + 1) - t0;
             const size_t off = t0 * rows_per_tile * row_bytes, len = nt * rows_per_tile * row_bytes;
             e = cudaStreamWaitEvent(copy_stream, done[c], 0);
             if (e != cudaSuccess) status = cuda_fail(e, "waiting for an output chunk");
