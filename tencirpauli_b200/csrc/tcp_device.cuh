@@ -20,7 +20,7 @@ constexpr uint32_t kTileBitsC128 = kLogThreads + kLogRowsC128;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s bound on any device wait
 constexpr uint32_t kCompensateGroups = 4;   // FP32: groups per Kahan fold
 
-constexpr uint32_t kPassBits = 2;            // host path: the state goes in as 4 parts
+constexpr uint32_t kPassBits = 3;            // host path: the state goes in by eighths of its tiles
 constexpr uint32_t kPassChunks = 1u << kPassBits;
 constexpr uint32_t kNoPasses = 0xffffffffu;
 
@@ -35,12 +35,12 @@ struct DevSchedule {
     const unsigned char *blocks64;   // step blocks with FP32 weights
     uint32_t nsteps;
     uint32_t tile_bits;
-    // Source-chunk passes of the host path: steps [pass_begin[v],
+    // Source-part passes of the host path: steps [pass_begin[v],
     // pass_begin[v + 1]) have outer patterns d whose top kPassBits bits equal
-    // v (steps are sorted by d), so in pass k an output tile t reads only
-    // source tiles t ^ d in the k-th of kPassChunks equal parts of the state
-    // when v = k ^ (t >> pass_shift).  pass_shift = kNoPasses when the state
-    // has fewer than kPassChunks tiles.
+    // v (steps are sorted by d), so an output tile t reads source tiles t ^ d
+    // in part v ^ (t >> pass_shift) of the kPassChunks equal parts of the
+    // state (pass_range).  pass_shift = kNoPasses when the state has fewer
+    // than kPassChunks tiles.
     uint32_t pass_begin[kPassChunks + 1];
     uint32_t pass_shift;
     // ring view (k_ring; see tcp::RingSchedule): ring_steps = 0 when the
@@ -59,6 +59,28 @@ struct DevSchedule {
     const float2 *t_wf;
     uint32_t ngroups;
 };
+
+// Step range [b0, b1) of host-path pass `pass` = p | log2(span) << 4 for
+// output tile `tile`: the pass reads the source parts of the aligned block
+// of `span` parts that contains part p, i.e. the steps whose top pattern bits
+// lie in the aligned block containing p ^ (tile >> shift), one contiguous
+// range since steps are sorted by d.  Constant indices only: a computed index
+// into the kernel's parameter struct would copy it to the stack.
+__device__ __forceinline__ void pass_range(const uint32_t (&begin)[kPassChunks + 1], uint32_t shift, uint64_t tile,
+                                           uint32_t pass, uint32_t &b0, uint32_t &b1) {
+    const uint32_t span = 1u << (pass >> 4);
+    const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> shift)) & (kPassChunks - 1u) & ~(span - 1u);
+    b0 = begin[0];
+    b1 = begin[kPassChunks];
+#pragma unroll
+    for (uint32_t w = 1; w < kPassChunks; ++w) {
+        if (v == w) b0 = begin[w];
+    }
+#pragma unroll
+    for (uint32_t w = 1; w < kPassChunks; ++w) {
+        if (v + span == w) b1 = begin[w];
+    }
+}
 
 // ------------------------------- PTX helpers -------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {

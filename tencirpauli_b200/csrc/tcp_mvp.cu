@@ -161,17 +161,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint64_t tile = tile0 + blockIdx.x;
     uint32_t step0 = 0, nsteps = s.nsteps;
     if constexpr (PASSES) {
-        // constant indices only: a computed index into the parameter struct
-        // would copy it to the stack
-        const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.pass_shift)) & (kPassChunks - 1u);
-        uint32_t b0 = s.pass_begin[0], b1 = s.pass_begin[1];
-#pragma unroll
-        for (uint32_t w = 1; w < kPassChunks; ++w) {
-            if (v == w) {
-                b0 = s.pass_begin[w];
-                b1 = s.pass_begin[w + 1];
-            }
-        }
+        uint32_t b0, b1;
+        pass_range(s.pass_begin, s.pass_shift, tile, pass, b0, b1);
         step0 = b0;
         nsteps = b1 - b0;
     }
@@ -314,15 +305,8 @@ __global__ void __launch_bounds__(RingShape<R>::kThreadsPerCta, 1)
     }
     uint32_t step0 = 0, nsteps = s.ring_steps;
     if constexpr (PASSES) {
-        const uint32_t v = (pass ^ static_cast<uint32_t>(tile >> s.ring_pass_shift)) & (kPassChunks - 1u);
-        uint32_t b0 = s.ring_pass_begin[0], b1 = s.ring_pass_begin[1];
-#pragma unroll
-        for (uint32_t w = 1; w < kPassChunks; ++w) {
-            if (v == w) {
-                b0 = s.ring_pass_begin[w];
-                b1 = s.ring_pass_begin[w + 1];
-            }
-        }
+        uint32_t b0, b1;
+        pass_range(s.ring_pass_begin, s.ring_pass_shift, tile, pass, b0, b1);
         step0 = b0;
         nsteps = b1 - b0;
     }
@@ -1100,27 +1084,34 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     cudaError_t e = status ? cudaSuccess : cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) status = cuda_fail(e, "cudaStreamCreate");
     // Large tiled applies overlap both copies with the kernel.
-    //  * Input: the state goes in as kPassChunks equal parts on its own
-    //    stream.  Pass k waits for part k only and runs the steps whose source
-    //    tiles lie in it (the kernels' `pass`), adding to y after the first,
-    //    so the copy of parts 1.. overlaps the earlier passes.
+    //  * Input: the state goes in as kParts parts on its own stream (an
+    //    eighth, an eighth, a quarter, a half).  Pass k waits for part k only
+    //    and runs the steps whose source tiles lie in it (the kernels'
+    //    `pass`), adding to y after the first, so the copy of parts 1..
+    //    overlaps the earlier passes.
     //  * Output: the first kFirstChunked passes run over every output tile;
-    //    the remaining ones run per chunk of consecutive output tiles
-    //    (chunk_start), all of a chunk's passes before the next chunk, and a
-    //    third stream copies each finished chunk of y to the host while the
-    //    next chunk computes.  The last chunks are smaller, so little copying
-    //    is left once the last kernel has finished (n = 28: 7-10 ms less).  Chunking the last two of four passes gives the
-    //    output copies half of the kernel time to overlap with (n = 28:
-    //    pageable 284 -> 257 ms, page-locked 261 -> 252 ms); chunking three
-    //    leaves the GPU waiting for the input staging.
+    //    the last one, half of the source, runs per chunk of consecutive
+    //    output tiles (chunk_start), and a third stream copies each finished
+    //    chunk of y to the host while the next chunk computes, so the output
+    //    copies overlap half of the kernel time.  The last chunks are
+    //    smaller, so little copying is left once the last kernel has
+    //    finished.
     // Every launch is queued right after the copy it waits for; ordinary
     // (pageable) buffers move through the staging ring (HostCopies).  Smaller
     // applies copy, launch once and copy back on one stream.
     const uint64_t tiles = tiled_tiles<R>(plan, ws.x);
     const uint64_t chunks = tiles >= kHostChunkTiles ? kHostChunks : 1;
     const bool passes = chunks > 1 && has_passes(plan, ws.x);
-    constexpr int kParts = static_cast<int>(kPassChunks);
-    constexpr int kFirstChunked = kParts - 2;  // passes run per output chunk from here on
+    // Source parts in eighths of the state's tiles: the input goes in as
+    // eighth 0, eighth 1, the second quarter and the second half; pass k
+    // reads exactly part k (kHostPass: base part | log2(parts) << 4), so the
+    // first kernel waits for one eighth of the state only.  The last pass,
+    // half of the source, runs per output chunk.
+    static_assert(kPassChunks == 8, "host passes are laid out in eighths");
+    constexpr int kParts = 4;
+    constexpr int kHostPass[kParts] = {0, 1, 2 | (1 << 4), 4 | (2 << 4)};
+    constexpr size_t kPartBegin[kParts + 1] = {0, 1, 2, 4, 8};  // eighths
+    constexpr int kFirstChunked = kParts - 1;  // passes run per output chunk from here on
     cudaStream_t copy_stream = nullptr, in_stream = nullptr;
     cudaEvent_t done[kHostChunks] = {};
     cudaEvent_t landed[kParts] = {};
@@ -1134,16 +1125,18 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
     }
     if (!status && chunks > 1) {
         if (passes) {
-            const size_t part = bytes / kParts;
+            const size_t eighth = bytes / kPassChunks;
             for (int k = 0; k < kParts && !status; ++k) {
-                status = copies.to_device(static_cast<unsigned char *>(ws.x) + k * part,
-                                          reinterpret_cast<const unsigned char *>(state) + k * part, part, in_stream);
+                const size_t off = kPartBegin[k] * eighth, len = (kPartBegin[k + 1] - kPartBegin[k]) * eighth;
+                status = copies.to_device(static_cast<unsigned char *>(ws.x) + off,
+                                          reinterpret_cast<const unsigned char *>(state) + off, len, in_stream);
                 if (!status) {
                     e = cudaEventRecord(landed[k], in_stream);
                     if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, landed[k], 0);
                     if (e != cudaSuccess) status = cuda_fail(e, "waiting for an input part");
                 }
-                if (!status && k < kFirstChunked) status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, k, k > 0);
+                if (!status && k < kFirstChunked)
+                    status = launch_one<R>(plan, ws.x, ws.y, stream, 0, 0, kHostPass[k], k > 0);
             }
         } else {
             status = copies.to_device(ws.x, state, bytes, stream);
@@ -1153,7 +1146,7 @@ int apply_host(const tcp_mvp_plan *plan, const R *state, uint64_t state_len, R *
             const uint64_t t0 = start(c), nt = start(c + 1) - t0;
             if (passes) {
                 for (int k = kFirstChunked; k < kParts && !status; ++k)
-                    status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, k, k > 0);
+                    status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt, kHostPass[k], k > 0);
             } else {
                 status = launch_one<R>(plan, ws.x, ws.y, stream, t0, nt);
             }
