@@ -440,6 +440,34 @@ def run_batched(args: argparse.Namespace) -> None:
         ref = oracle.apply_rows(op.nqubits, xm, zm, wp, xs[idx][nrhs - 1].cpu().numpy().astype(np.complex128), rows)
         got = ys[idx][nrhs - 1][torch.from_numpy(rows.astype(np.int64)).cuda()].cpu().numpy().astype(np.complex128)
         errs.append(float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+    smem_roofline = {
+        "bound": "smem",
+        "achieved": smem_ach / 1e12,
+        "peak": smem_rate / 1e12,
+        "unit": "TB/s",
+        "frac": smem_ach / smem_rate,
+        "traffic": None,
+        "peak_source": "tcp_probe_smem_rate on this GPU, best of 5",
+        "kernel": "k_ring (one launch per member, blockIdx.y = RHS)" if ring else "k_batched",
+        "smem_bytes_per_launch": smem_bytes,
+        "fp": {"achieved": flops / (ms / 1000.0) / 1e12, "peak": fma_rate / 1e12, "unit": "TFLOP/s",
+               "frac": flops / (ms / 1000.0) / fma_rate},
+        "hbm": {"achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "peak_source": peaks["source"]},
+    }
+    # The ring configuration is bound by instruction issue, as the
+    # single-vector kernel: its committed instruction count per apply (the
+    # 64 member launches) leads, shared memory, the FMA pipe and HBM beside it.
+    issue = (_issue_roofline("k_ring<float,rhs_block>", f"heisenberg{args.batch_count}_nmax{args.batch_nmax}_rhs{nrhs}_seed{args.seed}", ms,
+                             clocks) if ring else None)
+    if issue is not None:
+        batch_roofline = {"bound": "issue", **{k: issue[k] for k in ("achieved", "peak", "unit", "frac")}, "traffic": None,
+                          "kernel": smem_roofline["kernel"], "instructions_per_apply": issue["instructions_per_launch"],
+                          "peak_source": "4 warp instructions per SM clock x SMs x sampled SM clock; " + issue["source"],
+                          "smem": {k: v for k, v in smem_roofline.items() if k not in ("bound", "fp", "hbm", "kernel")},
+                          "fp": smem_roofline["fp"], "hbm": smem_roofline["hbm"]}
+    else:
+        batch_roofline = smem_roofline
     line = {
         "metric": METRIC,
         "value": amp_terms / (ms / 1000.0),
@@ -461,21 +489,7 @@ def run_batched(args: argparse.Namespace) -> None:
             "autotuned": tune,
             "l2": "inputs larger than L2, no flush",
         },
-        "roofline": {
-            "bound": "smem",
-            "achieved": smem_ach / 1e12,
-            "peak": smem_rate / 1e12,
-            "unit": "TB/s",
-            "frac": smem_ach / smem_rate,
-            "traffic": None,
-            "peak_source": "tcp_probe_smem_rate on this GPU, best of 5",
-            "kernel": "k_ring (one launch per member, blockIdx.y = RHS)" if ring else "k_batched",
-            "smem_bytes_per_launch": smem_bytes,
-            "fp": {"achieved": flops / (ms / 1000.0) / 1e12, "peak": fma_rate / 1e12, "unit": "TFLOP/s",
-                   "frac": flops / (ms / 1000.0) / fma_rate},
-            "hbm": {"achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                    "peak_source": peaks["source"]},
-        },
+        "roofline": batch_roofline,
         "e2e": None,
         "gpu_launches": args.steps * (tune["grid"] if ring else 1),
         "clocks": clocks,

@@ -25,6 +25,8 @@ def test_profile_counts_for_the_default_workloads() -> None:
     for lattice in ("4x6", "4x7"):
         count = bench._profile_instructions("k_u1_apply", f"j1j2_{lattice}_half_c128")
         assert count is not None and count > 1e8, lattice
+    count = bench._profile_instructions("k_ring<float,rhs_block>", "heisenberg64_nmax26_rhs8_seed20261203")
+    assert count is not None and count > 1e10
     assert bench._profile_instructions("k_ring<double>", "random2000_n99") is None
     traffic = bench._profile_traffic("k_ring<double>")
     # at least the compulsory bytes of one n = 28 launch (x read, y written)
