@@ -184,8 +184,9 @@ int tcp_mvp_apply_add_device(const tcp_mvp_plan *plan, const void *d_state, void
 
 /*
  * Batched MVP: many plans (Hamiltonians of uneven qubit and term counts), each
- * applied to a block of `nrhs` right-hand sides, in one persistent kernel
- * launch replayed from a CUDA graph.  No counterpart in the reference (its
+ * applied to a block of `nrhs` right-hand sides, replayed from one CUDA graph:
+ * one persistent kernel launch, or (the ring configuration below) one
+ * ring-kernel launch per member.  No counterpart in the reference (its
  * MvpPlan::apply_into, hamiltonian.rs:204-270, takes one state per call);
  * per vector the arithmetic is that of tcp_mvp_apply_into_device.
  * Buffers: d_x[h] / d_y[h] hold member h's nrhs vectors, RHS-major (vector v at
