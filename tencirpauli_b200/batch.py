@@ -1,10 +1,13 @@
 """Batched MVP over many Hamiltonians and right-hand-side blocks.
 
 ``BatchedMVP(plans, nrhs, dtype)`` applies every plan to its own block of
-``nrhs`` state vectors in one persistent kernel launch replayed from a CUDA
-graph (``tcp_mvp_batch_*`` in ``include/tcp_mvp.h``).  ``autotune`` times the
-kernel variants (tile rows x RHS block) on the caller's buffers and keeps the
-fastest, caching the choice on disk.
+``nrhs`` state vectors, replayed from one CUDA graph (``tcp_mvp_batch_*`` in
+``include/tcp_mvp.h``): either one persistent kernel launch over (member,
+tile, RHS block) work items, or -- the ring configuration (12, 1), the
+default when every member has at least 12 qubits -- one ring-kernel launch
+per member over all its tiles and right-hand sides.  ``autotune`` times the
+configurations (tile rows x RHS block, and the ring one) on the caller's
+buffers and keeps the fastest, caching the choice on disk.
 """
 
 from __future__ import annotations

@@ -1,7 +1,8 @@
 // libtcpmvp.so -- batched MVP: many Hamiltonians of uneven qubit and term
-// counts, each applied to a block of right-hand sides, in ONE persistent
-// launch that is captured in a CUDA graph, with tile shape and RHS block
-// picked by an autotuner (on-disk cache).
+// counts, each applied to a block of right-hand sides, replayed from one CUDA
+// graph, with the configuration picked by an autotuner (on-disk cache): one
+// persistent launch of k_batched (tile shape and RHS block), or the ring
+// configuration described below.
 //
 // k_batched<LOGT, RB, R>: persistent CTAs of 2^LOGT threads take work items
 // (Hamiltonian h, output tile of 2^LOGT rows, block of RB right-hand sides)
